@@ -1,0 +1,306 @@
+"""Benchmark of the fused stream-collide sweep on B200.
+
+Workload (default, one GPU): D3Q27 cumulant (Galilean-corrected, compressible), FP32, AA in-place
+streaming, 256 x 128 x 128 channel with NoSlip walls on the y and z faces, periodic in x, body
+force 1e-7 in x, omega = 1.95, rho = 1, velocity seeded uniform in +-1e-4.  A step is one sweep
+over the whole channel.  Metric: GLUPS (giga lattice-cell updates per second).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With torchrun (N > 1) every rank updates its own channel (replicas; the sweep has no data-path
+collective), and `value` is the sum over ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (256, 128, 128)
+Q = 27
+OMEGA = 1.95
+FORCE = 1e-7
+E2E_SWEEPS = 100          # sweeps per end-to-end call (one LatticeBoltzmannStep.run() in lbmpy terms)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def algorithmic_bytes_per_sweep(cells: int, q: int = Q, itemsize: int = 4) -> int:
+    """2 * Q * sizeof(PDF) per lattice update: every population read once and written once."""
+    return 2 * q * itemsize * cells
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while the timed region runs."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap"}
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.samples = []
+        self.reasons = set()
+        self._stop = threading.Event()
+        self._thread = None
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:   # NVML unavailable: report no samples
+            self._nv = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.01)
+
+    def __enter__(self):
+        if self._nv is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join()
+
+    def summary(self):
+        return {"sm_mhz": float(statistics.median(self.samples)) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def make_channel(device, shape=SHAPE, seed=0):
+    """The channel through the lbmpy-compatible API (create_channel-style set-up, AA in place)."""
+    import lbmpy_b200 as L
+    step = L.LatticeBoltzmannStep(domain_size=shape, periodicity=(True, False, False), stencil=L.Stencil.D3Q27,
+                                  method=L.Method.CUMULANT, relaxation_rate=OMEGA, compressible=True,
+                                  galilean_correction=True, force=(FORCE, 0, 0), streaming_pattern="aa",
+                                  config=L.CreateKernelConfig(data_type="float32"), device=device)
+    for d in ("N", "S", "T", "B"):
+        step.boundary_handling.set_boundary(L.NoSlip(), L.slice_from_direction(d, 3))
+    rng = np.random.default_rng(seed)
+    step.velocity_array[...] = rng.uniform(-1e-4, 1e-4, shape + (3,)).astype(np.float32)
+    step.set_pdf_fields_from_macroscopic_values()
+    return step
+
+
+def cpu_baseline_sample(seconds_budget=15.0):
+    """The oracle (C, OpenMP, FP64) on a bounded sample of the same channel: a 256 x 128 x 8
+    slab of the channel (periodic x, walls in y, z), timed on all host threads."""
+    from oracle import oracle as O
+    n = (256, 128, 8)
+    o = O.make("D3Q27", "cumulant", relaxation_rate=OMEGA, compressible=True, galilean_correction=True,
+               force=(FORCE, 0, 0))
+    f = o.new_field(n)
+    rng = np.random.default_rng(0)
+    o.set_equilibrium(f, np.ones(n), rng.uniform(-1e-4, 1e-4, n + (3,)), "aa", 1)
+    flags = np.zeros((n[0] + 2, n[1] + 2, n[2] + 2), np.uint8)
+    flags[:, 0, :] = flags[:, -1, :] = flags[:, :, 0] = flags[:, :, -1] = 1
+    par = 1
+    f, par = o.run(f, 1, "aa", par, periodic=(1, 0, 0), flags=flags)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        f, par = o.run(f, 2, "aa", par, periodic=(1, 0, 0), flags=flags)
+        steps += 2
+        if time.perf_counter() - t0 > seconds_budget / 3 or steps >= 40:
+            break
+    dt = time.perf_counter() - t0
+    cells = n[0] * n[1] * n[2]
+    return {"value": cells * steps / dt / 1e9, "unit": "GLUPS", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{steps} sweeps of a 256x128x8 slab of the channel (D3Q27 cumulant AA, FP64 oracle, "
+                      f"OpenMP)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    O.build()
+    n = (256, 128, 8)   # one bounded sample of the channel per step
+    o = O.make("D3Q27", "cumulant", relaxation_rate=OMEGA, compressible=True, galilean_correction=True,
+               force=(FORCE, 0, 0))
+    f = o.new_field(n)
+    rng = np.random.default_rng(0)
+    o.set_equilibrium(f, np.ones(n), rng.uniform(-1e-4, 1e-4, n + (3,)), "aa", 1)
+    flags = np.zeros((n[0] + 2, n[1] + 2, n[2] + 2), np.uint8)
+    flags[:, 0, :] = flags[:, -1, :] = flags[:, :, 0] = flags[:, :, -1] = 1
+    par = 1
+    for _ in range(args.warmup):
+        f, par = o.run(f, 1, "aa", par, periodic=(1, 0, 0), flags=flags)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        f, par = o.run(f, 1, "aa", par, periodic=(1, 0, 0), flags=flags)
+    dt = time.perf_counter() - t0
+    cells = n[0] * n[1] * n[2]
+    value = cells * args.steps / dt / 1e9
+    line = {"impl": "reference", "metric": "D3Q27 cumulant channel GLUPS", "value": value, "unit": "GLUPS",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "d3q27-cumulant-aa-channel-256x128x128 (sample: 256x128x8 slab per step)",
+                       "omega": OMEGA, "force": FORCE, "pattern": "aa", "galilean_correction": True},
+            "cpu_baseline": {"value": value, "unit": "GLUPS", "cores": os.cpu_count(), "kind": "port",
+                             "sample": "one sweep of a 256x128x8 slab of the channel per step (CPU oracle, "
+                                       "FP64, OpenMP on all host threads)"},
+            "e2e": {"value": value, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
+
+    from lbmpy_b200 import _native
+    _native.lib()
+    step = make_channel(device)
+    cells = SHAPE[0] * SHAPE[1] * SHAPE[2]
+    warm = max(args.warmup, 3)
+    for _ in range(warm + (warm % 2)):
+        step.time_step()
+    torch.cuda.synchronize()
+
+    stream = torch.cuda.current_stream()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step.time_step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = start.elapsed_time(stop)
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_per_step = ms_max / args.steps
+    glups = world * cells * args.steps / (ms_max * 1e-3) / 1e9
+
+    # roofline of the sweep kernel (the only kernel in the timed region)
+    peak, peak_kind = measured_peak()
+    achieved = algorithmic_bytes_per_sweep(cells) / (ms / args.steps * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            traffic = json.load(fh).get("d3q27_cumulant_aa_channel_fp32_bytes_per_launch")
+
+    # end to end through the public API: host PDFs in, run, PDFs and macroscopic fields out
+    e2e = None
+    if not args.no_e2e:
+        pdf_bytes = step.pdfs.untyped_storage().nbytes()
+        pinned = torch.empty(pdf_bytes // 4, dtype=torch.float32, pin_memory=True)
+        dev_flat = torch.empty(pdf_bytes // 4, dtype=torch.float32, device=device)
+        dev_flat.copy_(torch.as_strided(step.pdfs, (pdf_bytes // 4,), (1,), 0), non_blocking=False)
+        pinned.copy_(dev_flat)
+        vel_host = torch.empty(SHAPE + (3,), dtype=torch.float32, pin_memory=True)
+        rho_host = torch.empty(SHAPE, dtype=torch.float32, pin_memory=True)
+        import lbmpy_b200.macroscopic_value_kernels as mvk
+        vel_dev = torch.empty(SHAPE + (3,), dtype=torch.float32, device=device)
+        rho_dev = torch.empty(SHAPE, dtype=torch.float32, device=device)
+        storage = torch.as_strided(step.pdfs, (pdf_bytes // 4,), (1,), 0)
+        calls = 2
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(calls):
+            storage.copy_(pinned, non_blocking=True)              # host -> device PDFs
+            for _ in range(E2E_SWEEPS):
+                step.time_step()
+            mvk.get_macroscopic(step._macro, step.pdfs, rho_dev, vel_dev, step.previous_timestep)
+            pinned.copy_(storage, non_blocking=True)              # device -> host PDFs
+            vel_host.copy_(vel_dev, non_blocking=True)
+            rho_host.copy_(rho_dev, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=device)
+        if world > 1:
+            dist.all_reduce(ems, op=dist.ReduceOp.MAX)
+        e_glups = world * cells * E2E_SWEEPS * calls / (float(ems.item()) * 1e-3) / 1e9
+        e2e = {"value": e_glups, "unit": "GLUPS",
+               "h2d_bytes_per_step": int(pdf_bytes / E2E_SWEEPS),
+               "d2h_bytes_per_step": int((pdf_bytes + vel_host.numel() * 4 + rho_host.numel() * 4) / E2E_SWEEPS),
+               "sweeps_per_call": E2E_SWEEPS,
+               "call": "PDFs host->device, 100 x LatticeBoltzmannStep.time_step(), getter, PDFs+rho+u device->host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample()
+
+    if rank == 0:
+        line = {"metric": "D3Q27 cumulant channel GLUPS", "value": glups, "unit": "GLUPS", "n_gpus": world,
+                "steps": args.steps, "warmup": warm + (warm % 2), "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": "d3q27-cumulant-aa-channel-256x128x128", "shape": list(SHAPE),
+                           "omega": OMEGA, "force": FORCE, "pattern": "aa", "galilean_correction": True,
+                           "storage": "float32 zero-centred", "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2 (453 MB PDF field vs 126 MB L2)"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                             "bytes_per_lu": 2 * Q * 4},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
+                "clocks": clocks.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,134 @@
+/*
+ * lbm_b200.h -- C ABI of the B200 lattice Boltzmann sweep (liblbmb200.so).
+ *
+ * The library replaces the kernels that lbmpy generates and JIT-compiles through pystencils
+ * (paths relative to src/lbmpy of mabau/lbmpy).  Every entry point returns 0 on success and a
+ * non-zero LBM_E_* status otherwise; lbm_last_error() then holds a message.  All pointers
+ * passed as PDF / flag / macroscopic fields are device pointers owned by the caller; the
+ * library borrows them for the duration of the call.  Kernels are enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) and the calls return without waiting,
+ * except lbm_reduce_conserved, which waits for its result.
+ *
+ * PDF field layout (lbmpy's, creationfunctions.py:605-618 and updatekernels.py:146-163):
+ * interior domain nx*ny*nz plus one ghost layer per side, PDF index q in lbmpy's 'walberla'
+ * direction order (stencils.py:193-227).  Element (x, y, z, q) with x, y, z in [0, n+2)
+ * (ghost-inclusive coordinates) lives at  base + x + y*sy + z*sz + q*sq  elements; the x stride
+ * must be 1 and sy, sz, sq are passed in `strides` = {1, sy, sz, sq}.
+ *
+ * Flag field (optional): uint8 over the ghost-inclusive domain, x fastest, contiguous:
+ * index x + (nx+2)*(y + (ny+2)*z).  Low 3 bits: 0 fluid, 1 NoSlip, 2..5 UBB number 0..3;
+ * bit 7 marks fluid cells with a boundary neighbour (lbm_flags_finalize sets it).
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    LBM_OK = 0,
+    LBM_E_INVALID = 1,      /* argument rejected on the host (shape, stride, dtype, null pointer) */
+    LBM_E_CUDA = 2,         /* a CUDA call failed */
+    LBM_E_UNSUPPORTED = 3,  /* method / pattern / dtype combination not built */
+    LBM_E_DEVICE = 4        /* pointer or plan used on a different device than the plan's */
+};
+
+enum { LBM_STENCIL_D3Q19 = 19, LBM_STENCIL_D3Q27 = 27 };
+enum { LBM_METHOD_SRT = 0, LBM_METHOD_TRT = 1, LBM_METHOD_MRT = 2, LBM_METHOD_CUMULANT = 3 };
+enum { LBM_DTYPE_F64 = 0, LBM_DTYPE_F32 = 1, LBM_DTYPE_F16 = 2, LBM_DTYPE_BF16 = 3 };
+enum { LBM_PATTERN_PULL = 0, LBM_PATTERN_AA = 1, LBM_PATTERN_ESOTWIST = 2 };
+enum { LBM_FORCE_NONE = 0, LBM_FORCE_GUO = 1, LBM_FORCE_CENTRAL_MOMENT = 2, LBM_FORCE_SIMPLE = 3,
+       LBM_FORCE_LUO = 4 };
+enum { LBM_SGS_NONE = 0, LBM_SGS_SMAGORINSKY = 1 };
+
+/* Everything a sweep needs, resolved on the host by the lbmpy-compatible front end
+ * (LBMConfig.__post_init__, creationfunctions.py:347-484, and create_lb_method, :773-868). */
+typedef struct LbmPlanDesc {
+    int32_t stencil;            /* LBM_STENCIL_* */
+    int32_t method;             /* LBM_METHOD_* */
+    int32_t store_dtype;        /* LBM_DTYPE_*: PDF storage; arithmetic is FP64 for F64, else FP32 */
+    int32_t pattern;            /* LBM_PATTERN_* */
+    int32_t compressible;
+    int32_t continuous_equilibrium; /* SRT/TRT: 1 continuous Maxwellian (lbmpy default), 0 discrete */
+    double rates[27];           /* SRT: {w, w}; TRT: {w+, w-}; MRT / cumulant: one per moment in the
+                                   canonical order of the method's moment (cumulant) basis */
+    int32_t force_model;        /* LBM_FORCE_* */
+    double force[3];
+    int32_t galilean_correction;
+    int32_t sgs;                /* LBM_SGS_* */
+    double sgs_constant;
+    double shear_rate;          /* rate whose moments the SGS model adapts */
+    uint32_t sgs_mask;          /* bit k: moment k (SRT/TRT: bit0 even, bit1 odd) uses the shear rate */
+    double ubb_velocity[4][3];  /* wall velocity of UBB numbers 0..3 */
+    int32_t dims[3];            /* interior cells nx, ny, nz */
+    int32_t periodic[3];
+} LbmPlanDesc;
+
+typedef struct LbmPlan LbmPlan;
+
+/* Validates `desc` and prepares a plan on the current CUDA device.
+ * Replaces create_lb_function's code generation (creationfunctions.py:543-559). */
+int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out);
+int lbm_plan_destroy(LbmPlan* plan);
+
+/* Updates the physical parameters (rates, force, UBB velocities) of an existing plan without
+ * rebuilding it; the pystencils kernel took these as kernel keyword arguments
+ * (lbstep.py:269,280 `run_kernel(..., **kernel_params)`). */
+int lbm_plan_update(LbmPlan* plan, const LbmPlanDesc* desc);
+
+/* One fused stream-collide sweep.  Replaces the compiled kernel create_lb_function returns
+ * (creationfunctions.py:543-559), called as kernel(src=..., dst=...) by
+ * LatticeBoltzmannStep.time_step (lbstep.py:271-282), together with the boundary handling
+ * (boundaries/boundaryhandling.py:15-155) and periodic synchronisation it runs before the
+ * sweep.  Two-field pull: src != dst.  In-place AA / EsoTwist: src == dst and `parity` is the
+ * parity of THIS step (0 = EVEN, 1 = ODD; advanced_streaming/utility.py:18-38).
+ * omega_out (optional, float32, nx*ny*nz x-fastest) receives the effective shear rate. */
+int lbm_sweep(const LbmPlan* plan, const void* src, void* dst, const int64_t strides[4],
+              const uint8_t* flags, int parity, float* omega_out, void* stream);
+
+/* Runs `steps` sweeps; for pull the fields alternate a->b->a..., for in-place patterns
+ * `a` is updated starting at parity `first_parity`.  Sets *result_in_b for pull. */
+int lbm_run(const LbmPlan* plan, void* a, void* b, const int64_t strides[4], const uint8_t* flags,
+            int first_parity, int steps, int* result_in_b, void* stream);
+
+/* Equilibrium initialisation through the write accessor of the previous step
+ * (macroscopic_value_kernels.py:29-45, compile_macroscopic_values_setter :170-242).
+ * rho / u element type: double for F64 storage, float otherwise.  rho_strides: x, y, z;
+ * u_strides: x, y, z, component (elements). */
+int lbm_set_equilibrium(const LbmPlan* plan, void* pdfs, const int64_t strides[4], const void* rho,
+                        const int64_t rho_strides[3], const void* u, const int64_t u_strides[4],
+                        int prev_parity, void* stream);
+
+/* Density and velocity from the values the previous step wrote
+ * (macroscopic_value_kernels.py:48-61, compile_macroscopic_values_getter :88-167).
+ * rho or u may be NULL. */
+int lbm_get_macroscopic(const LbmPlan* plan, const void* pdfs, const int64_t strides[4], void* rho,
+                        const int64_t rho_strides[3], void* u, const int64_t u_strides[4],
+                        int prev_parity, void* stream);
+
+/* FP64 sums over fluid cells: out[0] mass, out[1..3] momentum (rho_ref * u incl. the force
+ * shift), out[4] kinetic energy.  No lbmpy counterpart (lbmpy reduces on the host through
+ * pystencils' data handling, lbstep.py:400); waits for the result. */
+int lbm_reduce_conserved(const LbmPlan* plan, const void* pdfs, const int64_t strides[4],
+                         const uint8_t* flags, int prev_parity, double out[5], void* stream);
+
+/* Sets bit 7 on every fluid cell of `flags` (device, layout above) that has a boundary
+ * neighbour along the plan's stencil, honouring periodicity.  Replaces the link-list setup of
+ * LatticeBoltzmannBoundaryHandling (boundaries/boundaryhandling.py:15-155). */
+int lbm_flags_finalize(const LbmPlan* plan, uint8_t* flags, void* stream);
+
+/* Copies the message of the last failed call on this thread into buf (NUL-terminated). */
+int lbm_last_error(char* buf, size_t n);
+
+/* Library version, for the loader's sanity check. */
+int lbm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H */

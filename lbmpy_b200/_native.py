@@ -1,0 +1,118 @@
+"""ctypes binding of liblbmb200.so (C ABI in include/lbm_b200.h).
+
+The library is built in-tree by ``python -m lbmpy_b200.build``.  There is no fallback: if the
+library is missing or a CUDA device is unavailable, every kernel call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblbmb200.so")
+
+LBM_OK, LBM_E_INVALID, LBM_E_CUDA, LBM_E_UNSUPPORTED, LBM_E_DEVICE = 0, 1, 2, 3, 4
+METHOD_SRT, METHOD_TRT, METHOD_MRT, METHOD_CUMULANT = 0, 1, 2, 3
+DTYPE_F64, DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2, 3
+PATTERN_PULL, PATTERN_AA, PATTERN_ESOTWIST = 0, 1, 2
+FORCE_NONE, FORCE_GUO, FORCE_CENTRAL_MOMENT, FORCE_SIMPLE, FORCE_LUO = 0, 1, 2, 3, 4
+SGS_NONE, SGS_SMAGORINSKY = 0, 1
+
+# exported symbols, one per declaration in include/lbm_b200.h
+EXPORTS = ("lbm_plan_create", "lbm_plan_destroy", "lbm_plan_update", "lbm_sweep", "lbm_run",
+           "lbm_set_equilibrium", "lbm_get_macroscopic", "lbm_reduce_conserved", "lbm_flags_finalize",
+           "lbm_last_error", "lbm_version")
+
+
+class LbmPlanDesc(ctypes.Structure):
+    _fields_ = [
+        ("stencil", ctypes.c_int32), ("method", ctypes.c_int32), ("store_dtype", ctypes.c_int32),
+        ("pattern", ctypes.c_int32), ("compressible", ctypes.c_int32),
+        ("continuous_equilibrium", ctypes.c_int32),
+        ("rates", ctypes.c_double * 27),
+        ("force_model", ctypes.c_int32),
+        ("force", ctypes.c_double * 3),
+        ("galilean_correction", ctypes.c_int32),
+        ("sgs", ctypes.c_int32),
+        ("sgs_constant", ctypes.c_double),
+        ("shear_rate", ctypes.c_double),
+        ("sgs_mask", ctypes.c_uint32),
+        ("ubb_velocity", (ctypes.c_double * 3) * 4),
+        ("dims", ctypes.c_int32 * 3),
+        ("periodic", ctypes.c_int32 * 3),
+    ]
+
+
+class LbmError(RuntimeError):
+    """A CUDA-side failure reported by liblbmb200."""
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m lbmpy_b200.build` "
+                              "(there is no CPU fallback for the B200 sweep)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)
+        L.lbm_plan_create.argtypes = [ctypes.POINTER(LbmPlanDesc), ctypes.POINTER(ctypes.c_void_p)]
+        L.lbm_plan_destroy.argtypes = [vp]
+        L.lbm_plan_update.argtypes = [vp, ctypes.POINTER(LbmPlanDesc)]
+        L.lbm_sweep.argtypes = [vp, vp, vp, i64p, vp, ctypes.c_int, vp, vp]
+        L.lbm_run.argtypes = [vp, vp, vp, i64p, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp]
+        L.lbm_set_equilibrium.argtypes = [vp, vp, i64p, vp, i64p, vp, i64p, ctypes.c_int, vp]
+        L.lbm_get_macroscopic.argtypes = [vp, vp, i64p, vp, i64p, vp, i64p, ctypes.c_int, vp]
+        L.lbm_reduce_conserved.argtypes = [vp, vp, i64p, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), vp]
+        L.lbm_flags_finalize.argtypes = [vp, vp, vp]
+        L.lbm_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        for name in EXPORTS:
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    lib().lbm_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, what: str = ""):
+    if rc == LBM_OK:
+        return
+    msg = last_error()
+    if what:
+        msg = f"{what}: {msg}"
+    if rc in (LBM_E_INVALID, LBM_E_DEVICE):
+        raise ValueError(msg)
+    if rc == LBM_E_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    raise LbmError(msg)
+
+
+def i64_array(values):
+    return (ctypes.c_int64 * len(values))(*[int(v) for v in values])
+
+
+class Plan:
+    """Owns an LbmPlan handle."""
+
+    def __init__(self, desc: LbmPlanDesc):
+        self.desc = desc
+        h = ctypes.c_void_p()
+        check(lib().lbm_plan_create(ctypes.byref(desc), ctypes.byref(h)), "lbm_plan_create")
+        self.handle = h
+
+    def update(self, desc: LbmPlanDesc):
+        check(lib().lbm_plan_update(self.handle, ctypes.byref(desc)), "lbm_plan_update")
+        self.desc = desc
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.lbm_plan_destroy(h)
+            self.handle = None

@@ -1,0 +1,82 @@
+"""Writes ``lbm_tables.h``: the compile-time lattice tables of the CUDA sweep.
+
+Run ``python -m lbmpy_b200.csrc.gen_tables`` (the build does it).  The tables come from
+``lbmpy_b200.methods`` (exact rationals) and are emitted as ``constexpr`` functions so that
+fully unrolled kernel loops fold every coefficient into the instruction stream; zero
+coefficients disappear at compile time.
+"""
+from __future__ import annotations
+
+import os
+from fractions import Fraction
+
+from lbmpy_b200 import methods as M
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _f(v) -> str:
+    v = Fraction(v)
+    if v.denominator == 1:
+        return f"{v.numerator}.0"
+    return repr(float(v))
+
+
+def _array_fn(name, values, rettype="double", nidx=1, dims=None):
+    flat = ", ".join(values)
+    if nidx == 1:
+        return (f"LBM_HD constexpr {rettype} {name}(int i) {{\n"
+                f"    constexpr {rettype} t[{len(values)}] = {{{flat}}};\n    return t[i];\n}}\n")
+    n0, n1 = dims
+    return (f"LBM_HD constexpr {rettype} {name}(int i, int j) {{\n"
+            f"    constexpr {rettype} t[{n0 * n1}] = {{{flat}}};\n    return t[i * {n1} + j];\n}}\n")
+
+
+def generate() -> str:
+    out = ["// Generated by gen_tables.py from lbmpy_b200/methods.py -- do not edit.",
+           "// Lattice tables of lbmpy's D3Q19 / D3Q27 methods in walberla direction order.",
+           "#pragma once", "",
+           "#ifndef LBM_HD", "#if defined(__CUDACC__)", "#define LBM_HD __host__ __device__ __forceinline__",
+           "#else", "#define LBM_HD inline", "#endif", "#endif", "",
+           "namespace lbm_tables {", ""]
+    for name in ("D3Q19", "D3Q27"):
+        q = len(M.directions(name))
+        dirs = M.directions(name)
+        inv = M.inverse_index(name)
+        w = M.weights(name)
+        pre = f"q{q}_"
+        out.append(f"// ---------------- {name}")
+        for d, axis in enumerate("xyz"):
+            out.append(_array_fn(pre + "c" + axis, [str(v[d]) for v in dirs], "int"))
+        out.append(_array_fn(pre + "inv", [str(v) for v in inv], "int"))
+        out.append(_array_fn(pre + "w", [_f(v) for v in w]))
+        for cont, tag in ((True, "cont"), (False, "disc")):
+            _, lin, quad = M.population_equilibrium(name, cont)
+            out.append(_array_fn(pre + "eqlin_" + tag, [_f(v) for r in lin for v in r], nidx=2, dims=(q, 3)))
+            out.append(_array_fn(pre + "eqquad_" + tag, [_f(v) for r in quad for v in r], nidx=2, dims=(q, 6)))
+        groups, Mm, Minv, eq = M.mrt_tables(name)
+        gid = [gi for gi, g in enumerate(groups) for _ in g]
+        out.append(f"constexpr int {pre}mrt_ngroups = {len(groups)};")
+        out.append(_array_fn(pre + "mrt_group", [str(v) for v in gid], "int"))
+        out.append(_array_fn(pre + "mrt_M", [_f(v) for r in Mm for v in r], nidx=2, dims=(q, q)))
+        out.append(_array_fn(pre + "mrt_Minv", [_f(v) for r in Minv for v in r], nidx=2, dims=(q, q)))
+        out.append(_array_fn(pre + "mrt_p0", [_f(e[0]) for e in eq]))
+        out.append(_array_fn(pre + "mrt_lin", [_f(v) for e in eq for v in e[1]], nidx=2, dims=(q, 3)))
+        out.append(_array_fn(pre + "mrt_quad", [_f(v) for e in eq for v in e[2]], nidx=2, dims=(q, 6)))
+        out.append("")
+    out.append("}  // namespace lbm_tables")
+    return "\n".join(out) + "\n"
+
+
+def write(path=None):
+    path = path or os.path.join(HERE, "lbm_tables.h")
+    text = generate()
+    old = open(path).read() if os.path.exists(path) else None
+    if old != text:
+        with open(path, "w") as f:
+            f.write(text)
+    return path
+
+
+if __name__ == "__main__":
+    print(write())

@@ -1,0 +1,467 @@
+// C ABI of liblbmb200.so (declared in include/lbm_b200.h): plan validation, launch
+// configuration and the macroscopic / reduction / flag kernels that do not depend on the method.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_dispatch.h"
+
+using namespace lbm;
+
+struct LbmPlan {
+    LbmPlanDesc desc;
+    int device;
+    int q, mk, store;
+    Physics phys;
+    double* partial;       // reduction scratch: RED_BLOCKS * 5 doubles
+    double* red_out;       // 5 doubles on the device
+    int red_blocks;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(LBM_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int check_device(const LbmPlan* p) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev != p->device)
+        return fail(LBM_E_DEVICE, "plan was created on device %d but device %d is current", p->device, dev);
+    return LBM_OK;
+}
+
+int check_device_ptr(const LbmPlan* p, const void* ptr, const char* name, bool nullable) {
+    if (ptr == nullptr) {
+        if (nullable) return LBM_OK;
+        return fail(LBM_E_INVALID, "%s is NULL", name);
+    }
+    cudaPointerAttributes at;
+    cudaError_t e = cudaPointerGetAttributes(&at, ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(LBM_E_INVALID, "%s is not a CUDA pointer", name);
+    }
+    if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+        return fail(LBM_E_INVALID, "%s must point to device memory", name);
+    if (at.device != p->device)
+        return fail(LBM_E_DEVICE, "%s lives on device %d, the plan on device %d", name, at.device, p->device);
+    return LBM_OK;
+}
+
+int check_strides(const LbmPlan* p, const int64_t s[4]) {
+    if (s == nullptr) return fail(LBM_E_INVALID, "strides is NULL");
+    const int64_t ex = p->desc.dims[0] + 2, ey = p->desc.dims[1] + 2, ez = p->desc.dims[2] + 2;
+    if (s[0] != 1) return fail(LBM_E_INVALID, "x stride must be 1 (fzyx layout), got %lld", (long long)s[0]);
+    if (s[1] < ex || s[2] < s[1] * ey || s[3] < s[2] * ez)
+        return fail(LBM_E_INVALID,
+                    "strides {%lld, %lld, %lld, %lld} overlap for a ghost-layered %lldx%lldx%lld field "
+                    "(need x fastest, then y, z, q)",
+                    (long long)s[0], (long long)s[1], (long long)s[2], (long long)s[3], (long long)ex,
+                    (long long)ey, (long long)ez);
+    if ((ex - 1) + (ey - 1) * s[1] + (ez - 1) * s[2] >= (int64_t(1) << 31))
+        return fail(LBM_E_INVALID, "one PDF slot plane must hold fewer than 2^31 elements");
+    return LBM_OK;
+}
+
+Grid make_grid(const LbmPlan* p, const int64_t s[4], const uint8_t* flags) {
+    Grid g;
+    g.nx = p->desc.dims[0];
+    g.ny = p->desc.dims[1];
+    g.nz = p->desc.dims[2];
+    g.sy = (int)s[1];
+    g.sz = (int)s[2];
+    g.sq = s[3];
+    g.periodic = (p->desc.periodic[0] ? 1 : 0) | (p->desc.periodic[1] ? 2 : 0) | (p->desc.periodic[2] ? 4 : 0);
+    g.flags = flags;
+    g.fsy = g.nx + 2;
+    g.fsz = (g.nx + 2) * (g.ny + 2);
+    return g;
+}
+
+void launch_shape(const Grid& g, dim3& grid, dim3& block) {
+    int bx = 32;
+    while (bx < g.nx && bx < 128) bx *= 2;
+    const int by = 256 / bx;
+    block = dim3(bx, by, 1);
+    grid = dim3((g.nx + bx - 1) / bx, (g.ny + by - 1) / by, g.nz);
+}
+
+int pattern_kind(const LbmPlan* p, int parity) {
+    switch (p->desc.pattern) {
+        case LBM_PATTERN_PULL: return PAT_PULL;
+        case LBM_PATTERN_AA: return parity ? PAT_AA_ODD : PAT_AA_EVEN;
+        case LBM_PATTERN_ESOTWIST: return parity ? PAT_ESO_ODD : PAT_ESO_EVEN;
+    }
+    return -1;
+}
+
+SweepLauncher sweep_launcher(const LbmPlan* p, int pat) {
+    if (p->q == 19 && p->mk == MK_POP) return sweep_q19_pop(p->store, pat);
+    if (p->q == 19 && p->mk == MK_MRT) return sweep_q19_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_POP) return sweep_q27_pop(p->store, pat);
+    if (p->q == 27 && p->mk == MK_MRT) return sweep_q27_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM) return sweep_q27_cum(p->store, pat);
+    return nullptr;
+}
+
+MacroLauncher set_eq_launcher(const LbmPlan* p, int pat) {
+    if (p->q == 19 && p->mk == MK_POP) return set_eq_q19_pop(p->store, pat);
+    if (p->q == 19 && p->mk == MK_MRT) return set_eq_q19_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_POP) return set_eq_q27_pop(p->store, pat);
+    if (p->q == 27 && p->mk == MK_MRT) return set_eq_q27_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM) return set_eq_q27_cum(p->store, pat);
+    return nullptr;
+}
+
+// ---- method-independent kernels, instantiated here
+template <class S, class R, int Q, int PAT>
+cudaError_t launch_get(const MacroArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
+    k_get_macroscopic<S, R, Q, PAT><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S, class R, int Q>
+MacroLauncher pick_get(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_get<S, R, Q, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_get<S, R, Q, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_get<S, R, Q, PAT_AA_ODD>;
+        case PAT_ESO_EVEN: return &launch_get<S, R, Q, PAT_ESO_EVEN>;
+        case PAT_ESO_ODD: return &launch_get<S, R, Q, PAT_ESO_ODD>;
+    }
+    return nullptr;
+}
+
+template <int Q>
+MacroLauncher get_launcher_q(int store, int pat) {
+    switch (store) {
+        case ST_F64: return pick_get<double, double, Q>(pat);
+        case ST_F32: return pick_get<float, float, Q>(pat);
+        case ST_F16: return pick_get<__half, float, Q>(pat);
+        case ST_BF16: return pick_get<__nv_bfloat16, float, Q>(pat);
+    }
+    return nullptr;
+}
+
+using ReduceLauncher = cudaError_t (*)(const MacroArgs&, int, double*, cudaStream_t);
+
+template <class S, int Q, int PAT>
+cudaError_t launch_reduce(const MacroArgs& a, int blocks, double* partial, cudaStream_t s) {
+    k_reduce_partial<S, Q, PAT><<<blocks, RED_THREADS, 0, s>>>(a, partial);
+    return cudaGetLastError();
+}
+
+template <class S, int Q>
+ReduceLauncher pick_reduce(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_reduce<S, Q, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_reduce<S, Q, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_reduce<S, Q, PAT_AA_ODD>;
+        case PAT_ESO_EVEN: return &launch_reduce<S, Q, PAT_ESO_EVEN>;
+        case PAT_ESO_ODD: return &launch_reduce<S, Q, PAT_ESO_ODD>;
+    }
+    return nullptr;
+}
+
+template <int Q>
+ReduceLauncher reduce_launcher_q(int store, int pat) {
+    switch (store) {
+        case ST_F64: return pick_reduce<double, Q>(pat);
+        case ST_F32: return pick_reduce<float, Q>(pat);
+        case ST_F16: return pick_reduce<__half, Q>(pat);
+        case ST_BF16: return pick_reduce<__nv_bfloat16, Q>(pat);
+    }
+    return nullptr;
+}
+
+// Marks fluid cells that have a boundary neighbour along the stencil.
+template <int Q>
+__global__ void k_flags_finalize(Grid g) {
+    using L = Lat<Q>;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.nx || y >= g.ny) return;
+    uint8_t* fl = const_cast<uint8_t*>(g.flags);
+    const int fc = (x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz;
+    int v = fl[fc] & ~FLAG_NEAR_WALL;
+    if ((v & FLAG_TYPE_MASK) == 0) {
+        Grid gf = g;
+        gf.sy = g.fsy;
+        gf.sz = g.fsz;
+        NbrOffsets nb;
+        nb.init(gf, x, y, z);
+        bool near = false;
+#pragma unroll
+        for (int i = 1; i < Q; ++i)
+            if (fl[fc + nb.off(L::cx(i), L::cy(i), L::cz(i))] & FLAG_TYPE_MASK) near = true;
+        if (near) v |= FLAG_NEAR_WALL;
+    }
+    fl[fc] = (uint8_t)v;
+}
+
+int fill_physics(LbmPlan* p, const LbmPlanDesc* d) {
+    Physics& ph = p->phys;
+    memset(&ph, 0, sizeof(ph));
+    for (int k = 0; k < 27; ++k) ph.rates[k] = d->rates[k];
+    for (int k = 0; k < 3; ++k) ph.force[k] = d->force[k];
+    ph.force_model = d->force_model;
+    ph.compressible = d->compressible ? 1 : 0;
+    ph.continuous_eq = d->continuous_equilibrium ? 1 : 0;
+    ph.sgs = d->sgs;
+    ph.sgs_c18 = 18.0 * d->sgs_constant * d->sgs_constant;
+    ph.tau0 = d->shear_rate != 0.0 ? 1.0 / d->shear_rate : 0.0;
+    ph.sgs_mask = d->sgs_mask;
+    ph.galilean = d->galilean_correction ? 1 : 0;
+    for (int u = 0; u < MAX_UBB; ++u)
+        for (int k = 0; k < 3; ++k) ph.ubb[u][k] = d->ubb_velocity[u][k];
+    if (d->method == LBM_METHOD_SRT) ph.rates[1] = ph.rates[0];
+    return LBM_OK;
+}
+
+int validate_desc(const LbmPlanDesc* d) {
+    if (d->stencil != 19 && d->stencil != 27) return fail(LBM_E_UNSUPPORTED, "stencil must be D3Q19 or D3Q27");
+    if (d->method < 0 || d->method > 3) return fail(LBM_E_INVALID, "unknown method %d", d->method);
+    if (d->method == LBM_METHOD_CUMULANT && d->stencil != 27)
+        return fail(LBM_E_UNSUPPORTED, "the cumulant sweep is built for D3Q27 only");
+    if (d->method == LBM_METHOD_CUMULANT && !d->compressible)
+        return fail(LBM_E_INVALID, "Incompressible cumulant-based methods are not supported (yet).");
+    if (d->store_dtype < 0 || d->store_dtype > 3) return fail(LBM_E_INVALID, "unknown dtype %d", d->store_dtype);
+    if (d->pattern < 0 || d->pattern > 2) return fail(LBM_E_INVALID, "unknown streaming pattern %d", d->pattern);
+    if (d->force_model < 0 || d->force_model > 4) return fail(LBM_E_INVALID, "unknown force model");
+    if (d->method == LBM_METHOD_CUMULANT && d->force_model != LBM_FORCE_NONE &&
+        d->force_model != LBM_FORCE_CENTRAL_MOMENT)
+        return fail(LBM_E_UNSUPPORTED, "the cumulant sweep supports the CentralMoment force model only");
+    if (d->method != LBM_METHOD_CUMULANT && d->force_model == LBM_FORCE_CENTRAL_MOMENT)
+        return fail(LBM_E_INVALID, "This force model can only be combined with the Cumulant collision model");
+    if (d->galilean_correction && d->method != LBM_METHOD_CUMULANT)
+        return fail(LBM_E_INVALID, "Galilean correction is only defined for D3Q27 cumulant methods.");
+    if (d->sgs != LBM_SGS_NONE && d->sgs != LBM_SGS_SMAGORINSKY) return fail(LBM_E_INVALID, "unknown SGS model");
+    if (d->sgs == LBM_SGS_SMAGORINSKY && !(d->shear_rate > 0.0))
+        return fail(LBM_E_INVALID, "the Smagorinsky model needs a positive shear relaxation rate");
+    for (int k = 0; k < 3; ++k)
+        if (d->dims[k] < 1) return fail(LBM_E_INVALID, "dims must be positive, got %d in axis %d", d->dims[k], k);
+    if (d->dims[1] > 65535 * 8 || d->dims[2] > 65535)
+        return fail(LBM_E_INVALID, "domain too large for the launch grid");
+    return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_version(void) { return 1; }
+
+int lbm_last_error(char* buf, size_t n) {
+    if (buf == nullptr || n == 0) return LBM_E_INVALID;
+    snprintf(buf, n, "%s", g_err.c_str());
+    return LBM_OK;
+}
+
+int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
+    if (desc == nullptr || out == nullptr) return fail(LBM_E_INVALID, "desc and out must not be NULL");
+    *out = nullptr;
+    int rc = validate_desc(desc);
+    if (rc) return rc;
+    LbmPlan* p = new LbmPlan();
+    p->desc = *desc;
+    cudaError_t e = cudaGetDevice(&p->device);
+    if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaGetDevice"); }
+    p->q = desc->stencil;
+    p->mk = desc->method == LBM_METHOD_MRT ? MK_MRT : (desc->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
+    p->store = desc->store_dtype;
+    fill_physics(p, desc);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
+    p->red_blocks = sms * 4;
+    e = cudaMalloc(&p->partial, sizeof(double) * 5 * (p->red_blocks + 1));
+    if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaMalloc(reduction scratch)"); }
+    p->red_out = p->partial + 5 * p->red_blocks;
+    if (sweep_launcher(p, PAT_PULL) == nullptr) {
+        cudaFree(p->partial);
+        delete p;
+        return fail(LBM_E_UNSUPPORTED, "no kernel built for this stencil/method/dtype");
+    }
+    *out = p;
+    return LBM_OK;
+}
+
+int lbm_plan_update(LbmPlan* p, const LbmPlanDesc* desc) {
+    if (p == nullptr || desc == nullptr) return fail(LBM_E_INVALID, "plan and desc must not be NULL");
+    if (desc->stencil != p->desc.stencil || desc->method != p->desc.method ||
+        desc->store_dtype != p->desc.store_dtype || desc->pattern != p->desc.pattern ||
+        memcmp(desc->dims, p->desc.dims, sizeof(desc->dims)) != 0)
+        return fail(LBM_E_INVALID, "lbm_plan_update may only change physical parameters");
+    int rc = validate_desc(desc);
+    if (rc) return rc;
+    p->desc = *desc;
+    fill_physics(p, desc);
+    return LBM_OK;
+}
+
+int lbm_plan_destroy(LbmPlan* p) {
+    if (p == nullptr) return LBM_OK;
+    if (p->partial) cudaFree(p->partial);
+    delete p;
+    return LBM_OK;
+}
+
+int lbm_sweep(const LbmPlan* p, const void* src, void* dst, const int64_t strides[4], const uint8_t* flags,
+              int parity, float* omega_out, void* stream) {
+    if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
+    int rc;
+    if ((rc = check_device(p))) return rc;
+    if ((rc = check_strides(p, strides))) return rc;
+    if ((rc = check_device_ptr(p, src, "src", false))) return rc;
+    if ((rc = check_device_ptr(p, dst, "dst", false))) return rc;
+    if ((rc = check_device_ptr(p, flags, "flags", true))) return rc;
+    if ((rc = check_device_ptr(p, omega_out, "omega_out", true))) return rc;
+    const bool inplace = p->desc.pattern != LBM_PATTERN_PULL;
+    if (inplace && src != dst) return fail(LBM_E_INVALID, "in-place streaming patterns need src == dst");
+    if (!inplace && src == dst) return fail(LBM_E_INVALID, "the pull pattern needs two distinct fields");
+    if (parity != 0 && parity != 1) return fail(LBM_E_INVALID, "parity must be 0 (EVEN) or 1 (ODD)");
+    const int pat = pattern_kind(p, parity);
+    SweepLauncher L = sweep_launcher(p, pat);
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no kernel for this pattern");
+    SweepArgs a;
+    a.g = make_grid(p, strides, flags);
+    a.p = p->phys;
+    a.src = src;
+    a.dst = dst;
+    a.omega_out = omega_out;
+    dim3 grid, block;
+    launch_shape(a.g, grid, block);
+    cudaError_t e = L(a, grid, block, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
+    return LBM_OK;
+}
+
+int lbm_run(const LbmPlan* p, void* a, void* b, const int64_t strides[4], const uint8_t* flags, int first_parity,
+            int steps, int* result_in_b, void* stream) {
+    if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
+    if (steps < 0) return fail(LBM_E_INVALID, "steps must be >= 0");
+    const bool inplace = p->desc.pattern != LBM_PATTERN_PULL;
+    void* src = a;
+    void* dst = inplace ? a : b;
+    int parity = first_parity;
+    int in_b = 0;
+    for (int t = 0; t < steps; ++t) {
+        int rc = lbm_sweep(p, src, dst, strides, flags, parity, nullptr, stream);
+        if (rc) return rc;
+        if (inplace) parity ^= 1;
+        else { void* tmp = src; src = dst; dst = tmp; in_b ^= 1; }
+    }
+    if (result_in_b) *result_in_b = in_b;
+    return LBM_OK;
+}
+
+static int macro_common(const LbmPlan* p, const void* pdfs, const int64_t strides[4], const void* rho,
+                        const int64_t rs[3], const void* u, const int64_t us[4], MacroArgs& a) {
+    int rc;
+    if ((rc = check_device(p))) return rc;
+    if ((rc = check_strides(p, strides))) return rc;
+    if ((rc = check_device_ptr(p, pdfs, "pdfs", false))) return rc;
+    if ((rc = check_device_ptr(p, rho, "rho", true))) return rc;
+    if ((rc = check_device_ptr(p, u, "u", true))) return rc;
+    if (rho && rs == nullptr) return fail(LBM_E_INVALID, "rho_strides is NULL");
+    if (u && us == nullptr) return fail(LBM_E_INVALID, "u_strides is NULL");
+    a.g = make_grid(p, strides, nullptr);
+    a.p = p->phys;
+    a.pdfs = const_cast<void*>(pdfs);
+    a.rho = const_cast<void*>(rho);
+    a.u = const_cast<void*>(u);
+    for (int k = 0; k < 3; ++k) a.rs[k] = rho ? rs[k] : 0;
+    for (int k = 0; k < 4; ++k) a.us[k] = u ? us[k] : 0;
+    return LBM_OK;
+}
+
+int lbm_set_equilibrium(const LbmPlan* p, void* pdfs, const int64_t strides[4], const void* rho,
+                        const int64_t rho_strides[3], const void* u, const int64_t u_strides[4], int prev_parity,
+                        void* stream) {
+    if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
+    if (rho == nullptr || u == nullptr) return fail(LBM_E_INVALID, "rho and u are required");
+    MacroArgs a;
+    int rc = macro_common(p, pdfs, strides, rho, rho_strides, u, u_strides, a);
+    if (rc) return rc;
+    MacroLauncher L = set_eq_launcher(p, pattern_kind(p, prev_parity ? 1 : 0));
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no setter kernel");
+    dim3 grid, block;
+    launch_shape(a.g, grid, block);
+    cudaError_t e = L(a, grid, block, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "setter launch");
+}
+
+int lbm_get_macroscopic(const LbmPlan* p, const void* pdfs, const int64_t strides[4], void* rho,
+                        const int64_t rho_strides[3], void* u, const int64_t u_strides[4], int prev_parity,
+                        void* stream) {
+    if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
+    MacroArgs a;
+    int rc = macro_common(p, pdfs, strides, rho, rho_strides, u, u_strides, a);
+    if (rc) return rc;
+    const int pat = pattern_kind(p, prev_parity ? 1 : 0);
+    MacroLauncher L = p->q == 19 ? get_launcher_q<19>(p->store, pat) : get_launcher_q<27>(p->store, pat);
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no getter kernel");
+    dim3 grid, block;
+    launch_shape(a.g, grid, block);
+    cudaError_t e = L(a, grid, block, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "getter launch");
+}
+
+int lbm_reduce_conserved(const LbmPlan* p, const void* pdfs, const int64_t strides[4], const uint8_t* flags,
+                         int prev_parity, double out[5], void* stream) {
+    if (p == nullptr || out == nullptr) return fail(LBM_E_INVALID, "plan and out must not be NULL");
+    MacroArgs a;
+    int rc = macro_common(p, pdfs, strides, nullptr, nullptr, nullptr, nullptr, a);
+    if (rc) return rc;
+    if ((rc = check_device_ptr(p, flags, "flags", true))) return rc;
+    a.g.flags = flags;
+    const int pat = pattern_kind(p, prev_parity ? 1 : 0);
+    ReduceLauncher L = p->q == 19 ? reduce_launcher_q<19>(p->store, pat) : reduce_launcher_q<27>(p->store, pat);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = L(a, p->red_blocks, p->partial, s);
+    if (e != cudaSuccess) return cuda_fail(e, "reduction launch");
+    k_reduce_finish<<<1, 32, 0, s>>>(p->partial, p->red_blocks, p->red_out);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "reduction finish launch");
+    e = cudaMemcpyAsync(out, p->red_out, 5 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(e, "reduction copy");
+    e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "reduction sync");
+}
+
+int lbm_flags_finalize(const LbmPlan* p, uint8_t* flags, void* stream) {
+    if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
+    int rc;
+    if ((rc = check_device(p))) return rc;
+    if ((rc = check_device_ptr(p, flags, "flags", false))) return rc;
+    int64_t s[4] = {1, p->desc.dims[0] + 2, (int64_t)(p->desc.dims[0] + 2) * (p->desc.dims[1] + 2), 0};
+    Grid g = make_grid(p, s, flags);
+    dim3 grid, block;
+    launch_shape(g, grid, block);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (p->q == 19) k_flags_finalize<19><<<grid, block, 0, st>>>(g);
+    else k_flags_finalize<27><<<grid, block, 0, st>>>(g);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "flag finalize launch");
+}
+
+}  // extern "C"

@@ -1,0 +1,454 @@
+// Per-cell collision operators of lbmpy's methods, written for registers.
+//
+// All operators work on zero-centred PDFs f~ = f - w (lbmpy's default storage,
+// creationfunctions.py:140) and return post-collision PDFs in place.
+//   collide_pop  -- SRT/TRT in population space, delta equilibrium
+//                   (methods/momentbased/momentbasedmethod.py:389-398)
+//   collide_mrt  -- raw-moment MRT with the weighted-orthogonal basis
+//                   (methods/momentbased/momentbasedmethod.py:359-387)
+//   collide_cum  -- D3Q27 polynomial cumulants (Geier et al. 2015) with optional Galilean
+//                   correction and CentralMoment forcing
+//                   (methods/cumulantbased/cumulantbasedmethod.py:296-402,
+//                    methods/cumulantbased/galilean_correction.py:56-91, forcemodels.py:213-233)
+// Smagorinsky (turbulence_models.py:25-84) is shared by all three.
+#pragma once
+#include "lbm_common.cuh"
+
+namespace lbm {
+
+// acc + c*x for a compile-time table coefficient c: zeros and unit factors fold away
+// (IEEE arithmetic forbids the compiler from dropping 0*x on its own).
+template <class R>
+__device__ __forceinline__ R cmad(R acc, double c, R x) {
+    return c == 0.0 ? acc : (c == 1.0 ? acc + x : (c == -1.0 ? acc - x : acc + R(c) * x));
+}
+
+// Conserved quantities of zero-centred PDFs (methods/conservedquantitycomputation.py:218-249).
+template <int Q, class R> struct Macro {
+    R drho, rho, rho_ref, ux, uy, uz;
+};
+
+template <int Q, class R>
+__device__ __forceinline__ Macro<Q, R> conserved(const R (&f)[Q], const Physics& p, bool eq_shift) {
+    using L = Lat<Q>;
+    R d = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        d += f[i];
+        if (L::cx(i) == 1) jx += f[i]; else if (L::cx(i) == -1) jx -= f[i];
+        if (L::cy(i) == 1) jy += f[i]; else if (L::cy(i) == -1) jy -= f[i];
+        if (L::cz(i) == 1) jz += f[i]; else if (L::cz(i) == -1) jz -= f[i];
+    }
+    Macro<Q, R> m;
+    m.drho = d;
+    m.rho = R(1) + d;
+    m.rho_ref = p.compressible ? m.rho : R(1);
+    const R inv = R(1) / m.rho_ref;
+    m.ux = jx * inv; m.uy = jy * inv; m.uz = jz * inv;
+    if (eq_shift) {
+        const R h = R(0.5) * inv;
+        m.ux += h * R(p.force[0]); m.uy += h * R(p.force[1]); m.uz += h * R(p.force[2]);
+    }
+    return m;
+}
+
+// Smagorinsky rate from the non-equilibrium stress.  f_eq's second raw moments are
+// rho_f*u_a*u_b + delta_ab*drho/3 for every method here (they are matched moments).
+template <int Q, class R>
+__device__ __forceinline__ R smagorinsky_rate(const R (&f)[Q], const Macro<Q, R>& m, const Physics& p) {
+    using L = Lat<Q>;
+    R sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        if (L::cx(i) != 0) sxx += f[i];
+        if (L::cy(i) != 0) syy += f[i];
+        if (L::cz(i) != 0) szz += f[i];
+        if (L::cx(i) * L::cy(i) == 1) sxy += f[i]; else if (L::cx(i) * L::cy(i) == -1) sxy -= f[i];
+        if (L::cx(i) * L::cz(i) == 1) sxz += f[i]; else if (L::cx(i) * L::cz(i) == -1) sxz -= f[i];
+        if (L::cy(i) * L::cz(i) == 1) syz += f[i]; else if (L::cy(i) * L::cz(i) == -1) syz -= f[i];
+    }
+    const R rf = p.compressible ? m.rho : R(1);
+    const R third = m.drho * R(1.0 / 3.0);
+    const R pxx = sxx - rf * m.ux * m.ux - third;
+    const R pyy = syy - rf * m.uy * m.uy - third;
+    const R pzz = szz - rf * m.uz * m.uz - third;
+    const R pxy = sxy - rf * m.ux * m.uy;
+    const R pxz = sxz - rf * m.ux * m.uz;
+    const R pyz = syz - rf * m.uy * m.uz;
+    const R s2 = pxx * pxx + pyy * pyy + pzz * pzz + R(2) * (pxy * pxy + pxz * pxz + pyz * pyz);
+    const R pi = sqrt(R(2) * s2) / m.rho_ref;
+    const R tau0 = R(p.tau0);
+    return R(2) / (tau0 + sqrt(R(p.sgs_c18) * pi + tau0 * tau0));
+}
+
+// ------------------------------------------------------------------ SRT / TRT
+template <int Q, class R>
+__device__ __forceinline__ R collide_pop(R (&f)[Q], const Physics& p) {
+    using L = Lat<Q>;
+    const bool shift = p.force_model == FM_GUO || p.force_model == FM_CENTRAL;
+    const Macro<Q, R> m = conserved<Q, R>(f, p, shift);
+    R wp = R(p.rates[0]), wm = R(p.rates[1]);
+    if (p.sgs == 1) {
+        const R om = smagorinsky_rate<Q, R>(f, m, p);
+        if (p.sgs_mask & 1u) wp = om;
+        if (p.sgs_mask & 2u) wm = om;
+    }
+    const R rf = p.compressible ? m.rho : R(1);
+    const R uxx = m.ux * m.ux, uyy = m.uy * m.uy, uzz = m.uz * m.uz;
+    const R uxy = m.ux * m.uy, uxz = m.ux * m.uz, uyz = m.uy * m.uz;
+    const bool cont = p.continuous_eq != 0;
+    const bool has_force = p.force_model == FM_GUO || p.force_model == FM_SIMPLE || p.force_model == FM_LUO;
+    const R Fx = R(p.force[0]), Fy = R(p.force[1]), Fz = R(p.force[2]);
+    const R uF = m.ux * Fx + m.uy * Fy + m.uz * Fz;
+    R fe_scale = R(1), fo_scale = R(1), fe_on = R(1);
+    if (p.force_model == FM_GUO) { fe_scale = R(1) - R(0.5) * wp; fo_scale = R(1) - R(0.5) * wm; }
+    if (p.force_model == FM_SIMPLE) fe_on = R(0);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int j = L::inv(i);
+        if (j < i) continue;   // handle each (i, inverse) pair once
+        const R w = R(L::w(i));
+        R quad = 0;
+        if (cont) {
+            quad = cmad(quad, L::eqquad(true, i, 0), uxx); quad = cmad(quad, L::eqquad(true, i, 1), uyy);
+            quad = cmad(quad, L::eqquad(true, i, 2), uzz); quad = cmad(quad, L::eqquad(true, i, 3), uxy);
+            quad = cmad(quad, L::eqquad(true, i, 4), uxz); quad = cmad(quad, L::eqquad(true, i, 5), uyz);
+        } else {
+            quad = cmad(quad, L::eqquad(false, i, 0), uxx); quad = cmad(quad, L::eqquad(false, i, 1), uyy);
+            quad = cmad(quad, L::eqquad(false, i, 2), uzz); quad = cmad(quad, L::eqquad(false, i, 3), uxy);
+            quad = cmad(quad, L::eqquad(false, i, 4), uxz); quad = cmad(quad, L::eqquad(false, i, 5), uyz);
+        }
+        const R feq_e = m.drho * w + rf * quad;
+        R force_e = 0, force_o = 0;
+        if (has_force) {
+            const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
+            const R cu = R(L::cx(i)) * m.ux + R(L::cy(i)) * m.uy + R(L::cz(i)) * m.uz;
+            force_e = fe_on * fe_scale * w * (R(9) * cF * cu - R(3) * uF);
+            force_o = fo_scale * w * R(3) * cF;
+        }
+        if (j == i) {   // rest direction: even only
+            f[i] = f[i] + wp * (feq_e - f[i]) + force_e;
+        } else {
+            R lin = 0;
+            lin = cmad(lin, L::eqlin(true, i, 0), m.ux);
+            lin = cmad(lin, L::eqlin(true, i, 1), m.uy);
+            lin = cmad(lin, L::eqlin(true, i, 2), m.uz);
+            const R feq_o = rf * lin;
+            const R fi = f[i], fj = f[j];
+            const R fe = R(0.5) * (fi + fj), fo = R(0.5) * (fi - fj);
+            const R de = wp * (feq_e - fe) + force_e;
+            const R dod = wm * (feq_o - fo) + force_o;
+            f[i] = fi + de + dod;
+            f[j] = fj + de - dod;
+        }
+    }
+    return wp;
+}
+
+// ------------------------------------------------------------------ MRT (raw moment space)
+template <int Q, class R>
+__device__ __forceinline__ R collide_mrt(R (&f)[Q], const Physics& p) {
+    using L = Lat<Q>;
+    const bool shift = p.force_model == FM_GUO || p.force_model == FM_CENTRAL;
+    const Macro<Q, R> m = conserved<Q, R>(f, p, shift);
+    R om_sgs = R(0);
+    if (p.sgs == 1) om_sgs = smagorinsky_rate<Q, R>(f, m, p);
+    const R rf = p.compressible ? m.rho : R(1);
+    const R uu[6] = {m.ux * m.ux, m.uy * m.uy, m.uz * m.uz, m.ux * m.uy, m.ux * m.uz, m.uy * m.uz};
+    const bool has_force = p.force_model == FM_GUO || p.force_model == FM_SIMPLE || p.force_model == FM_LUO;
+    R luo[Q];
+    if (has_force) {
+        const R Fx = R(p.force[0]), Fy = R(p.force[1]), Fz = R(p.force[2]);
+        const R uF = m.ux * Fx + m.uy * Fy + m.uz * Fz;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
+            const R cu = R(L::cx(i)) * m.ux + R(L::cy(i)) * m.uy + R(L::cz(i)) * m.uz;
+            luo[i] = p.force_model == FM_SIMPLE ? R(L::w(i)) * R(3) * cF
+                                                : R(L::w(i)) * (R(9) * cF * cu + R(3) * cF - R(3) * uF);
+        }
+    }
+    R delta[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        R mk = 0;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) mk = cmad(mk, L::M(k, i), f[i]);
+        R lin = 0, quad = 0;
+        lin = cmad(lin, L::mlin(k, 0), m.ux);
+        lin = cmad(lin, L::mlin(k, 1), m.uy);
+        lin = cmad(lin, L::mlin(k, 2), m.uz);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) quad = cmad(quad, L::mquad(k, a), uu[a]);
+        const R meq = cmad(rf * (lin + quad), L::p0(k), m.drho);
+        R r = R(p.rates[k]);
+        if (p.sgs == 1 && ((p.sgs_mask >> k) & 1u)) r = om_sgs;
+        R d = r * (meq - mk);
+        if (has_force) {
+            R fk = 0;
+#pragma unroll
+            for (int i = 0; i < Q; ++i) fk = cmad(fk, L::M(k, i), luo[i]);
+            if (p.force_model == FM_GUO) fk *= (R(1) - R(0.5) * r);
+            d += fk;
+        }
+        delta[k] = d;
+    }
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        R s = 0;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) s = cmad(s, L::Minv(i, k), delta[k]);
+        f[i] += s;
+    }
+    return p.sgs == 1 ? om_sgs : R(0);
+}
+
+// ------------------------------------------------------------------ D3Q27 cumulant
+// Index of direction i in the 3x3x3 velocity cube, (cx+1)*9 + (cy+1)*3 + (cz+1).
+template <int Q> LBM_HD constexpr int cube(int i) {
+    return (Lat<Q>::cx(i) + 1) * 9 + (Lat<Q>::cy(i) + 1) * 3 + (Lat<Q>::cz(i) + 1);
+}
+
+// Forward: populations on the velocity cube -> central moments about u, axis by axis.
+template <class R>
+__device__ __forceinline__ void chimera_forward(R (&g)[27], R u, int stride, int s1, int s2) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const int base = a * s1 + b * s2;
+            const R fm = g[base], f0 = g[base + stride], fp = g[base + 2 * stride];
+            const R k0 = fm + f0 + fp;
+            const R dm = fp - fm;
+            const R k1 = dm - u * k0;
+            const R k2 = (fp + fm) - R(2) * u * dm + u * u * k0;
+            g[base] = k0; g[base + stride] = k1; g[base + 2 * stride] = k2;
+        }
+    }
+}
+
+// Backward: central moments about u -> populations, axis by axis.
+template <class R>
+__device__ __forceinline__ void chimera_backward(R (&g)[27], R u, int stride, int s1, int s2) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const int base = a * s1 + b * s2;
+            const R k0 = g[base], k1 = g[base + stride], k2 = g[base + 2 * stride];
+            const R m1 = k1 + u * k0;
+            const R m2 = k2 + R(2) * u * k1 + u * u * k0;
+            g[base] = R(0.5) * (m2 - m1);
+            g[base + stride] = k0 - m2;
+            g[base + 2 * stride] = R(0.5) * (m2 + m1);
+        }
+    }
+}
+
+template <class R>
+__device__ __forceinline__ R collide_cum(R (&f)[27], const Physics& p) {
+    using L = Lat<27>;
+    const bool cm_force = p.force_model == FM_CENTRAL;
+    const Macro<27, R> m = conserved<27, R>(f, p, cm_force);
+    const R rho = m.rho, irho = R(1) / rho;
+    const R ux = m.ux, uy = m.uy, uz = m.uz;
+    R om_sgs = R(0);
+    if (p.sgs == 1) om_sgs = smagorinsky_rate<27, R>(f, m, p);
+
+    R k[27];
+#pragma unroll
+    for (int i = 0; i < 27; ++i) k[cube<27>(i)] = f[i];
+    chimera_forward(k, uz, 1, 9, 3);   // z moments
+    chimera_forward(k, uy, 3, 9, 1);   // y moments
+    chimera_forward(k, ux, 9, 3, 1);   // x moments
+    // background (lattice weights) central moments are separable: B0 = 1, B1 = -u, B2 = 1/3 + u^2
+    const R bx[3] = {R(1), -ux, R(1.0 / 3.0) + ux * ux};
+    const R by[3] = {R(1), -uy, R(1.0 / 3.0) + uy * uy};
+    const R bz[3] = {R(1), -uz, R(1.0 / 3.0) + uz * uz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) k[a * 9 + b * 3 + c] += bx[a] * by[b] * bz[c];
+    // conserved central moments after the symmetric forcing step are exact: rho and 0
+#define K(a, b, c) k[(a) * 9 + (b) * 3 + (c)]
+    K(0, 0, 0) = rho; K(1, 0, 0) = 0; K(0, 1, 0) = 0; K(0, 0, 1) = 0;
+
+    // ---- monomial cumulants (rho-scaled), zero first-order central moments
+    const R k200 = K(2, 0, 0), k020 = K(0, 2, 0), k002 = K(0, 0, 2);
+    const R k110 = K(1, 1, 0), k101 = K(1, 0, 1), k011 = K(0, 1, 1);
+    const R k111 = K(1, 1, 1), k210 = K(2, 1, 0), k201 = K(2, 0, 1), k120 = K(1, 2, 0);
+    const R k021 = K(0, 2, 1), k102 = K(1, 0, 2), k012 = K(0, 1, 2);
+    const R C220 = K(2, 2, 0) - (k200 * k020 + R(2) * k110 * k110) * irho;
+    const R C202 = K(2, 0, 2) - (k200 * k002 + R(2) * k101 * k101) * irho;
+    const R C022 = K(0, 2, 2) - (k020 * k002 + R(2) * k011 * k011) * irho;
+    const R C211 = K(2, 1, 1) - (k200 * k011 + R(2) * k110 * k101) * irho;
+    const R C121 = K(1, 2, 1) - (k020 * k101 + R(2) * k110 * k011) * irho;
+    const R C112 = K(1, 1, 2) - (k002 * k110 + R(2) * k101 * k011) * irho;
+    const R C122 = K(1, 2, 2) - (k020 * k102 + k002 * k120 + R(2) * k110 * k012 + R(2) * k101 * k021 +
+                                 R(4) * k011 * k111) * irho;
+    const R C212 = K(2, 1, 2) - (k200 * k012 + k002 * k210 + R(2) * k110 * k102 + R(4) * k101 * k111 +
+                                 R(2) * k011 * k201) * irho;
+    const R C221 = K(2, 2, 1) - (k200 * k021 + k020 * k201 + R(4) * k110 * k111 + R(2) * k101 * k120 +
+                                 R(2) * k011 * k210) * irho;
+    const R C222 = K(2, 2, 2) -
+                   (k200 * K(0, 2, 2) + k020 * K(2, 0, 2) + k002 * K(2, 2, 0) +
+                    R(4) * (k110 * K(1, 1, 2) + k101 * K(1, 2, 1) + k011 * K(2, 1, 1))) * irho -
+                   (R(2) * (k210 * k012 + k201 * k021 + k120 * k102) + R(4) * k111 * k111) * irho +
+                   R(2) * (k200 * k020 * k002 + R(2) * (k200 * k011 * k011 + k020 * k101 * k101 +
+                                                        k002 * k110 * k110) + R(8) * k110 * k101 * k011) *
+                       irho * irho;
+
+    // ---- relaxation of the polynomial cumulants (group rates from the plan)
+    auto rate = [&](int idx) -> R {
+        R r = R(p.rates[idx]);
+        if (p.sgs == 1 && ((p.sgs_mask >> idx) & 1u)) r = om_sgs;
+        return r;
+    };
+    // canonical order (methods.cumulant_groups): 0 rho | 1-3 momentum | 4 xy 5 xz 6 yz 7 x2-y2 8 x2-z2 |
+    // 9 bulk | 10-12 (xy2+xz2, x2y+yz2, x2z+y2z) | 13-15 differences | 16 xyz | 17-18 | 19 | 20-22 | 23-25 | 26
+    const R w_xy = rate(4), w_xz = rate(5), w_yz = rate(6), w_d1 = rate(7), w_d2 = rate(8), w_b = rate(9);
+    const R P_d1 = k200 - k020, P_d2 = k200 - k002, P_b = k200 + k020 + k002;
+    R Ps_d1 = P_d1 - w_d1 * P_d1;
+    R Ps_d2 = P_d2 - w_d2 * P_d2;
+    R Ps_b = P_b + w_b * (rho - P_b);
+    const R c110 = k110 - w_xy * k110, c101 = k101 - w_xz * k101, c011 = k011 - w_yz * k011;
+    if (p.galilean) {
+        const R o1 = R(p.rates[7]), o2 = R(p.rates[9]);   // base rates, not the SGS-adapted ones
+        const R h = R(0.5) * irho;
+        const R Dx = -o1 * h * (R(2) * k200 - k020 - k002) - o2 * h * (k200 + k020 + k002 - rho);
+        const R Dy = Dx + R(3) * o1 * h * (k200 - k020);
+        const R Dz = Dx + R(3) * o1 * h * (k200 - k002);
+        const R a1 = R(-3) * rho * (R(1) - R(0.5) * o1);
+        const R a2 = R(-3) * rho * (R(1) - R(0.5) * o2);
+        Ps_d1 += a1 * (ux * ux * Dx - uy * uy * Dy);
+        Ps_d2 += a1 * (ux * ux * Dx - uz * uz * Dz);
+        Ps_b += a2 * (ux * ux * Dx + uy * uy * Dy + uz * uz * Dz);
+    }
+    const R c200 = (Ps_b + Ps_d1 + Ps_d2) * R(1.0 / 3.0);
+    const R c020 = c200 - Ps_d1;
+    const R c002 = c200 - Ps_d2;
+    // third order: sums and differences relax separately, xyz alone
+    const R s1 = (k120 + k102) * (R(1) - rate(10)), s2 = (k210 + k012) * (R(1) - rate(11)),
+            s3 = (k201 + k021) * (R(1) - rate(12));
+    const R d1 = (k120 - k102) * (R(1) - rate(13)), d2 = (k210 - k012) * (R(1) - rate(14)),
+            d3 = (k201 - k021) * (R(1) - rate(15));
+    const R c111 = k111 * (R(1) - rate(16));
+    const R c120 = R(0.5) * (s1 + d1), c102 = R(0.5) * (s1 - d1);
+    const R c210 = R(0.5) * (s2 + d2), c012 = R(0.5) * (s2 - d2);
+    const R c201 = R(0.5) * (s3 + d3), c021 = R(0.5) * (s3 - d3);
+    // fourth order
+    const R q1 = (C220 - R(2) * C202 + C022) * (R(1) - rate(17));
+    const R q2 = (C220 + C202 - R(2) * C022) * (R(1) - rate(18));
+    const R q3 = (C220 + C202 + C022) * (R(1) - rate(19));
+    const R C220s = (q3 + q1 + q2) * R(1.0 / 3.0);
+    const R C202s = (q3 - q1) * R(1.0 / 3.0);
+    const R C022s = (q3 - q2) * R(1.0 / 3.0);
+    const R C211s = C211 * (R(1) - rate(20)), C121s = C121 * (R(1) - rate(21)), C112s = C112 * (R(1) - rate(22));
+    const R C221s = C221 * (R(1) - rate(23)), C212s = C212 * (R(1) - rate(24)), C122s = C122 * (R(1) - rate(25));
+    const R C222s = C222 * (R(1) - rate(26));
+
+    // ---- back to central moments (moment-cumulant relations, zero first order)
+    K(2, 0, 0) = c200; K(0, 2, 0) = c020; K(0, 0, 2) = c002;
+    K(1, 1, 0) = c110; K(1, 0, 1) = c101; K(0, 1, 1) = c011;
+    K(1, 1, 1) = c111; K(2, 1, 0) = c210; K(2, 0, 1) = c201; K(1, 2, 0) = c120;
+    K(0, 2, 1) = c021; K(1, 0, 2) = c102; K(0, 1, 2) = c012;
+    const R k220s = C220s + (c200 * c020 + R(2) * c110 * c110) * irho;
+    const R k202s = C202s + (c200 * c002 + R(2) * c101 * c101) * irho;
+    const R k022s = C022s + (c020 * c002 + R(2) * c011 * c011) * irho;
+    K(2, 2, 0) = k220s; K(2, 0, 2) = k202s; K(0, 2, 2) = k022s;
+    K(2, 1, 1) = C211s + (c200 * c011 + R(2) * c110 * c101) * irho;
+    K(1, 2, 1) = C121s + (c020 * c101 + R(2) * c110 * c011) * irho;
+    K(1, 1, 2) = C112s + (c002 * c110 + R(2) * c101 * c011) * irho;
+    K(1, 2, 2) = C122s + (c020 * c102 + c002 * c120 + R(2) * c110 * c012 + R(2) * c101 * c021 +
+                          R(4) * c011 * c111) * irho;
+    K(2, 1, 2) = C212s + (c200 * c012 + c002 * c210 + R(2) * c110 * c102 + R(4) * c101 * c111 +
+                          R(2) * c011 * c201) * irho;
+    K(2, 2, 1) = C221s + (c200 * c021 + c020 * c201 + R(4) * c110 * c111 + R(2) * c101 * c120 +
+                          R(2) * c011 * c210) * irho;
+    K(2, 2, 2) = C222s +
+                 (c200 * C022s + c020 * C202s + c002 * C220s +
+                  R(4) * (c110 * C112s + c101 * C121s + c011 * C211s)) * irho +
+                 (R(2) * (c210 * c012 + c201 * c021 + c120 * c102) + R(4) * c111 * c111) * irho +
+                 (c200 * c020 * c002 + R(2) * (c200 * c011 * c011 + c020 * c101 * c101 + c002 * c110 * c110) +
+                  R(8) * c110 * c101 * c011) * irho * irho;
+    // symmetric forcing, second half: first-order central moments become F/2
+    if (cm_force) {
+        K(1, 0, 0) = R(0.5) * R(p.force[0]);
+        K(0, 1, 0) = R(0.5) * R(p.force[1]);
+        K(0, 0, 1) = R(0.5) * R(p.force[2]);
+    }
+#undef K
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) k[a * 9 + b * 3 + c] -= bx[a] * by[b] * bz[c];
+    chimera_backward(k, ux, 9, 3, 1);
+    chimera_backward(k, uy, 3, 9, 1);
+    chimera_backward(k, uz, 1, 9, 3);
+#pragma unroll
+    for (int i = 0; i < 27; ++i) f[i] = k[cube<27>(i)];
+    return p.sgs == 1 ? om_sgs : R(p.rates[4]);
+}
+
+// ------------------------------------------------------------------ equilibria (setter)
+// Zero-centred equilibrium populations of the method at (rho, u) (macroscopic_value_kernels.py:29-45).
+template <int Q, class R, int MK>
+__device__ __forceinline__ void equilibrium(R (&f)[Q], R rho, R ux, R uy, R uz, const Physics& p) {
+    using L = Lat<Q>;
+    const R drho = rho - R(1);
+    if (MK == MK_CUM) {
+        // product form: kappa = rho * Gaussian moments (variance 1/3), shifted by u
+        const R phx[3] = {R(0.5) * (R(1.0 / 3.0) + ux * ux - ux), R(2.0 / 3.0) - ux * ux,
+                          R(0.5) * (R(1.0 / 3.0) + ux * ux + ux)};
+        const R phy[3] = {R(0.5) * (R(1.0 / 3.0) + uy * uy - uy), R(2.0 / 3.0) - uy * uy,
+                          R(0.5) * (R(1.0 / 3.0) + uy * uy + uy)};
+        const R phz[3] = {R(0.5) * (R(1.0 / 3.0) + uz * uz - uz), R(2.0 / 3.0) - uz * uz,
+                          R(0.5) * (R(1.0 / 3.0) + uz * uz + uz)};
+#pragma unroll
+        for (int i = 0; i < Q; ++i)
+            f[i] = rho * phx[L::cx(i) + 1] * phy[L::cy(i) + 1] * phz[L::cz(i) + 1] - R(L::w(i));
+        return;
+    }
+    const R rf = p.compressible ? rho : R(1);
+    const R uu[6] = {ux * ux, uy * uy, uz * uz, ux * uy, ux * uz, uy * uz};
+    if (MK == MK_MRT) {
+        // f = M^-1 m_eq with the MRT basis (identical to the population form of the same equilibrium)
+        R meq[Q];
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            R lin = 0, quad = 0;
+            lin = cmad(lin, L::mlin(k, 0), ux);
+            lin = cmad(lin, L::mlin(k, 1), uy);
+            lin = cmad(lin, L::mlin(k, 2), uz);
+#pragma unroll
+            for (int a = 0; a < 6; ++a) quad = cmad(quad, L::mquad(k, a), uu[a]);
+            meq[k] = cmad(rf * (lin + quad), L::p0(k), drho);
+        }
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            R s = 0;
+#pragma unroll
+            for (int k = 0; k < Q; ++k) s = cmad(s, L::Minv(i, k), meq[k]);
+            f[i] = s;
+        }
+        return;
+    }
+    const bool cont = p.continuous_eq != 0;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        R lin = 0, quad = 0;
+        lin = cmad(lin, L::eqlin(true, i, 0), ux);
+        lin = cmad(lin, L::eqlin(true, i, 1), uy);
+        lin = cmad(lin, L::eqlin(true, i, 2), uz);
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+            quad = cont ? cmad(quad, L::eqquad(true, i, a), uu[a]) : cmad(quad, L::eqquad(false, i, a), uu[a]);
+        f[i] = drho * R(L::w(i)) + rf * (lin + quad);
+    }
+}
+
+}  // namespace lbm

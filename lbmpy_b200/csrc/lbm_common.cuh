@@ -1,0 +1,135 @@
+// Shared definitions of the B200 lattice Boltzmann sweep: lattice traits, PDF storage
+// conversions and the by-value argument block every kernel receives.
+#pragma once
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "lbm_tables.h"
+
+namespace lbm {
+
+enum StoreType : int { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3 };
+enum MethodKind : int { MK_POP = 0, MK_MRT = 1, MK_CUM = 2 };   // SRT/TRT | raw-moment MRT | cumulant
+enum PatternKind : int { PAT_PULL = 0, PAT_AA_EVEN = 1, PAT_AA_ODD = 2, PAT_ESO_EVEN = 3, PAT_ESO_ODD = 4 };
+enum ForceKind : int { FM_NONE = 0, FM_GUO = 1, FM_CENTRAL = 2, FM_SIMPLE = 3, FM_LUO = 4 };
+
+// Cell flags (uint8, ghost-layered domain): low 3 bits = cell type, bit 7 = fluid cell with at
+// least one boundary neighbour.  Type 0 fluid, 1 NoSlip, 2..5 UBB number (type - 2).
+constexpr int FLAG_TYPE_MASK = 7;
+constexpr int FLAG_NEAR_WALL = 128;
+constexpr int FLAG_NOSLIP = 1;
+constexpr int FLAG_UBB0 = 2;
+constexpr int MAX_UBB = 4;
+
+template <int Q> struct Lat;
+
+template <> struct Lat<19> {
+    static constexpr int Q = 19;
+    LBM_HD static constexpr int cx(int i) { return lbm_tables::q19_cx(i); }
+    LBM_HD static constexpr int cy(int i) { return lbm_tables::q19_cy(i); }
+    LBM_HD static constexpr int cz(int i) { return lbm_tables::q19_cz(i); }
+    LBM_HD static constexpr int inv(int i) { return lbm_tables::q19_inv(i); }
+    LBM_HD static constexpr double w(int i) { return lbm_tables::q19_w(i); }
+    LBM_HD static constexpr double eqlin(bool cont, int i, int a) {
+        return cont ? lbm_tables::q19_eqlin_cont(i, a) : lbm_tables::q19_eqlin_disc(i, a);
+    }
+    LBM_HD static constexpr double eqquad(bool cont, int i, int a) {
+        return cont ? lbm_tables::q19_eqquad_cont(i, a) : lbm_tables::q19_eqquad_disc(i, a);
+    }
+    LBM_HD static constexpr double M(int k, int i) { return lbm_tables::q19_mrt_M(k, i); }
+    LBM_HD static constexpr double Minv(int i, int k) { return lbm_tables::q19_mrt_Minv(i, k); }
+    LBM_HD static constexpr double p0(int k) { return lbm_tables::q19_mrt_p0(k); }
+    LBM_HD static constexpr double mlin(int k, int a) { return lbm_tables::q19_mrt_lin(k, a); }
+    LBM_HD static constexpr double mquad(int k, int a) { return lbm_tables::q19_mrt_quad(k, a); }
+};
+
+template <> struct Lat<27> {
+    static constexpr int Q = 27;
+    LBM_HD static constexpr int cx(int i) { return lbm_tables::q27_cx(i); }
+    LBM_HD static constexpr int cy(int i) { return lbm_tables::q27_cy(i); }
+    LBM_HD static constexpr int cz(int i) { return lbm_tables::q27_cz(i); }
+    LBM_HD static constexpr int inv(int i) { return lbm_tables::q27_inv(i); }
+    LBM_HD static constexpr double w(int i) { return lbm_tables::q27_w(i); }
+    LBM_HD static constexpr double eqlin(bool cont, int i, int a) {
+        return cont ? lbm_tables::q27_eqlin_cont(i, a) : lbm_tables::q27_eqlin_disc(i, a);
+    }
+    LBM_HD static constexpr double eqquad(bool cont, int i, int a) {
+        return cont ? lbm_tables::q27_eqquad_cont(i, a) : lbm_tables::q27_eqquad_disc(i, a);
+    }
+    LBM_HD static constexpr double M(int k, int i) { return lbm_tables::q27_mrt_M(k, i); }
+    LBM_HD static constexpr double Minv(int i, int k) { return lbm_tables::q27_mrt_Minv(i, k); }
+    LBM_HD static constexpr double p0(int k) { return lbm_tables::q27_mrt_p0(k); }
+    LBM_HD static constexpr double mlin(int k, int a) { return lbm_tables::q27_mrt_lin(k, a); }
+    LBM_HD static constexpr double mquad(int k, int a) { return lbm_tables::q27_mrt_quad(k, a); }
+};
+
+// ------------------------------------------------------------------ storage conversions
+template <class S, class R> struct Conv;
+template <class R> struct Conv<double, R> {
+    __device__ __forceinline__ static R ld(const double* p) { return (R)*p; }
+    __device__ __forceinline__ static void st(double* p, R v) { *p = (double)v; }
+};
+template <class R> struct Conv<float, R> {
+    __device__ __forceinline__ static R ld(const float* p) { return (R)*p; }
+    __device__ __forceinline__ static void st(float* p, R v) { *p = (float)v; }
+};
+template <class R> struct Conv<__half, R> {
+    __device__ __forceinline__ static R ld(const __half* p) { return (R)__half2float(*p); }
+    __device__ __forceinline__ static void st(__half* p, R v) { *p = __float2half_rn((float)v); }
+};
+template <class R> struct Conv<__nv_bfloat16, R> {
+    __device__ __forceinline__ static R ld(const __nv_bfloat16* p) { return (R)__bfloat162float(*p); }
+    __device__ __forceinline__ static void st(__nv_bfloat16* p, R v) { *p = __float2bfloat16_rn((float)v); }
+};
+
+// ------------------------------------------------------------------ kernel arguments
+struct Physics {
+    double rates[27];      // per moment (MRT), per polynomial cumulant, or [omega+, omega-] (SRT/TRT)
+    double force[3];
+    int force_model;
+    int compressible;
+    int continuous_eq;     // SRT/TRT equilibrium: continuous Maxwellian (1) or discrete (0)
+    int sgs;               // 0 none, 1 Smagorinsky
+    double sgs_c18;        // 18 * C^2
+    double tau0;           // 1 / shear rate
+    uint32_t sgs_mask;     // moments (or TRT parts) whose rate is the shear rate
+    int galilean;
+    double ubb[MAX_UBB][3];
+};
+
+struct Grid {
+    int nx, ny, nz;        // interior cells
+    int sy, sz;            // element strides of y and z (x stride is 1)
+    long long sq;          // element stride between PDF slots
+    int periodic;          // bit 0 x, bit 1 y, bit 2 z
+    const uint8_t* flags;  // (nx+2)*(ny+2)*(nz+2), x fastest, or nullptr
+    int fsy, fsz;          // flag strides
+};
+
+struct SweepArgs {
+    Grid g;
+    Physics p;
+    const void* src;
+    void* dst;
+    float* omega_out;      // optional per-cell effective shear rate (interior, x fastest)
+};
+
+// Neighbour offsets in elements for c in {-1, 0, +1} along each axis, with periodic wrap.
+struct NbrOffsets {
+    int dx[3], dy[3], dz[3];
+    __device__ __forceinline__ void init(const Grid& g, int x, int y, int z) {
+        dx[1] = 0; dy[1] = 0; dz[1] = 0;
+        dx[0] = (x == 0 && (g.periodic & 1)) ? g.nx - 1 : -1;
+        dx[2] = (x == g.nx - 1 && (g.periodic & 1)) ? -(g.nx - 1) : 1;
+        dy[0] = ((y == 0 && (g.periodic & 2)) ? g.ny - 1 : -1) * g.sy;
+        dy[2] = ((y == g.ny - 1 && (g.periodic & 2)) ? -(g.ny - 1) : 1) * g.sy;
+        dz[0] = ((z == 0 && (g.periodic & 4)) ? g.nz - 1 : -1) * g.sz;
+        dz[2] = ((z == g.nz - 1 && (g.periodic & 4)) ? -(g.nz - 1) : 1) * g.sz;
+    }
+    __device__ __forceinline__ int off(int cx, int cy, int cz) const {
+        return dx[cx + 1] + dy[cy + 1] + dz[cz + 1];
+    }
+};
+
+}  // namespace lbm

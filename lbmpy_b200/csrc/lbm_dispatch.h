@@ -1,0 +1,111 @@
+// Launcher tables: one instantiated kernel per (stencil, method, storage type, pattern).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lbm_kernels.cuh"
+
+namespace lbm {
+
+using SweepLauncher = cudaError_t (*)(const SweepArgs&, dim3, dim3, cudaStream_t);
+using MacroLauncher = cudaError_t (*)(const MacroArgs&, dim3, dim3, cudaStream_t);
+
+template <class S, class R, int Q, int MK, int PAT>
+cudaError_t launch_sweep(const SweepArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
+    k_sweep<S, R, Q, MK, PAT><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S, class R, int Q, int MK, int PAT>
+cudaError_t launch_set_eq(const MacroArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
+    k_set_equilibrium<S, R, Q, MK, PAT><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S, class R, int Q, int MK>
+SweepLauncher pick_sweep_pattern(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_sweep<S, R, Q, MK, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_sweep<S, R, Q, MK, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_sweep<S, R, Q, MK, PAT_AA_ODD>;
+        case PAT_ESO_EVEN: return &launch_sweep<S, R, Q, MK, PAT_ESO_EVEN>;
+        case PAT_ESO_ODD: return &launch_sweep<S, R, Q, MK, PAT_ESO_ODD>;
+    }
+    return nullptr;
+}
+
+template <class S, class R, int Q, int MK>
+MacroLauncher pick_set_eq_pattern(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_set_eq<S, R, Q, MK, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_set_eq<S, R, Q, MK, PAT_AA_ODD>;
+        case PAT_ESO_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_ESO_EVEN>;
+        case PAT_ESO_ODD: return &launch_set_eq<S, R, Q, MK, PAT_ESO_ODD>;
+    }
+    return nullptr;
+}
+
+// Instantiates the sweep and setter families of one (Q, method) pair in one translation unit.
+#define LBM_DEFINE_FAMILY(NAME, Q, MK)                                                          \
+    SweepLauncher sweep_##NAME(int store, int pat) {                                            \
+        switch (store) {                                                                        \
+            case ST_F64: return pick_sweep_pattern<double, double, Q, MK>(pat);                  \
+            case ST_F32: return pick_sweep_pattern<float, float, Q, MK>(pat);                    \
+            case ST_F16: return pick_sweep_pattern<__half, float, Q, MK>(pat);                   \
+            case ST_BF16: return pick_sweep_pattern<__nv_bfloat16, float, Q, MK>(pat);          \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    MacroLauncher set_eq_##NAME(int store, int pat) {                                           \
+        switch (store) {                                                                        \
+            case ST_F64: return pick_set_eq_pattern<double, double, Q, MK>(pat);                 \
+            case ST_F32: return pick_set_eq_pattern<float, float, Q, MK>(pat);                   \
+            case ST_F16: return pick_set_eq_pattern<__half, float, Q, MK>(pat);                  \
+            case ST_BF16: return pick_set_eq_pattern<__nv_bfloat16, float, Q, MK>(pat);         \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }
+
+// Reduced family (FP64 / FP32 storage, pull and AA): for bases whose fully unrolled 27x27
+// transforms make every extra instantiation expensive to compile.
+#define LBM_DEFINE_FAMILY_REDUCED(NAME, Q, MK)                                                  \
+    template <class S, class R>                                                                 \
+    static SweepLauncher NAME##_sweep_pat(int pat) {                                            \
+        switch (pat) {                                                                          \
+            case PAT_PULL: return &launch_sweep<S, R, Q, MK, PAT_PULL>;                         \
+            case PAT_AA_EVEN: return &launch_sweep<S, R, Q, MK, PAT_AA_EVEN>;                   \
+            case PAT_AA_ODD: return &launch_sweep<S, R, Q, MK, PAT_AA_ODD>;                     \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    template <class S, class R>                                                                 \
+    static MacroLauncher NAME##_set_pat(int pat) {                                              \
+        switch (pat) {                                                                          \
+            case PAT_PULL: return &launch_set_eq<S, R, Q, MK, PAT_PULL>;                        \
+            case PAT_AA_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_AA_EVEN>;                  \
+            case PAT_AA_ODD: return &launch_set_eq<S, R, Q, MK, PAT_AA_ODD>;                    \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    SweepLauncher sweep_##NAME(int store, int pat) {                                            \
+        if (store == ST_F64) return NAME##_sweep_pat<double, double>(pat);                      \
+        if (store == ST_F32) return NAME##_sweep_pat<float, float>(pat);                        \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    MacroLauncher set_eq_##NAME(int store, int pat) {                                           \
+        if (store == ST_F64) return NAME##_set_pat<double, double>(pat);                        \
+        if (store == ST_F32) return NAME##_set_pat<float, float>(pat);                          \
+        return nullptr;                                                                         \
+    }
+
+#define LBM_DECLARE_FAMILY(NAME)                   \
+    SweepLauncher sweep_##NAME(int store, int pat); \
+    MacroLauncher set_eq_##NAME(int store, int pat);
+
+LBM_DECLARE_FAMILY(q19_pop)
+LBM_DECLARE_FAMILY(q19_mrt)
+LBM_DECLARE_FAMILY(q27_pop)
+LBM_DECLARE_FAMILY(q27_mrt)
+LBM_DECLARE_FAMILY(q27_cum)
+
+}  // namespace lbm

@@ -1,0 +1,287 @@
+// Kernels of the B200 lattice Boltzmann sweep.
+//
+// k_sweep: one fused stream-collide update of every fluid cell, one thread per cell, SoA
+// (fzyx) PDF layout, x fastest.  The PDF accessors follow lbmpy's fieldaccess.py:66-181:
+//   pull      read src[x - c_i](i)            write dst[x](i)
+//   AA even   read f[x](i)                    write f[x](inv i)
+//   AA odd    read f[x - c_i](inv i)          write f[x + c_i](i)
+//   EsoTwist  even/odd with offsets max(-c,0) / max(c,0) (fieldaccess.py:160-181)
+// Periodicity is an index wrap instead of ghost-layer copies, and NoSlip / UBB bounce-back
+// (boundaries/boundaryconditions.py:128-139, 794-841) is fused into the read: where lbmpy's
+// boundary kernel would have written the wall slot, the sweep reads the value that kernel
+// would have copied (the f_out location of advanced_streaming/indexing.py:12-183).
+#pragma once
+#include "lbm_collide.cuh"
+
+namespace lbm {
+
+template <int PAT> struct Access {
+    // read location of direction i: offset (ox, oy, oz) and slot
+    template <int Q>
+    LBM_HD static constexpr int rslot(int i) {
+        return (PAT == PAT_AA_ODD || PAT == PAT_ESO_ODD) ? Lat<Q>::inv(i) : i;
+    }
+    template <int Q>
+    LBM_HD static constexpr int roff(int i, int d) {
+        const int c = d == 0 ? Lat<Q>::cx(i) : (d == 1 ? Lat<Q>::cy(i) : Lat<Q>::cz(i));
+        return PAT == PAT_PULL ? -c
+             : PAT == PAT_AA_EVEN ? 0
+             : PAT == PAT_AA_ODD ? -c
+             : (c < 0 ? -c : 0);   // EsoTwist: max(-c, 0)
+    }
+    template <int Q>
+    LBM_HD static constexpr int wslot(int i) {
+        return (PAT == PAT_AA_EVEN || PAT == PAT_ESO_EVEN) ? Lat<Q>::inv(i) : i;
+    }
+    template <int Q>
+    LBM_HD static constexpr int woff(int i, int d) {
+        const int c = d == 0 ? Lat<Q>::cx(i) : (d == 1 ? Lat<Q>::cy(i) : Lat<Q>::cz(i));
+        return PAT == PAT_PULL ? 0
+             : PAT == PAT_AA_EVEN ? 0
+             : PAT == PAT_AA_ODD ? c
+             : (c > 0 ? c : 0);    // EsoTwist: max(c, 0)
+    }
+};
+
+// Write pattern of the previous step (where f_out lives) for the current pattern.
+template <int PAT> struct PrevPattern {
+    static constexpr int value = PAT == PAT_AA_EVEN ? PAT_AA_ODD
+                               : PAT == PAT_AA_ODD ? PAT_AA_EVEN
+                               : PAT == PAT_ESO_EVEN ? PAT_ESO_ODD
+                               : PAT == PAT_ESO_ODD ? PAT_ESO_EVEN
+                               : PAT_PULL;
+};
+
+template <class R, int Q, int MK>
+__device__ __forceinline__ R collide(R (&f)[Q], const Physics& p) {
+    if constexpr (MK == MK_POP) return collide_pop<Q, R>(f, p);
+    else if constexpr (MK == MK_MRT) return collide_mrt<Q, R>(f, p);
+    else return collide_cum<R>(f, p);
+}
+
+// Fused bounce-back for a fluid cell next to a boundary: replaces the pulled value of every
+// direction whose source cell x - c_i is a wall.
+template <class S, class R, int Q, int PAT>
+__device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const NbrOffsets& nb, int cell,
+                                         int x, int y, int z) {
+    using L = Lat<Q>;
+    using PA = Access<PrevPattern<PAT>::value>;
+    const Grid& g = a.g;
+    const S* src = static_cast<const S*>(a.src);
+    NbrOffsets fo;
+    {
+        Grid gf = g;
+        gf.sy = g.fsy; gf.sz = g.fsz;
+        fo.init(gf, x, y, z);
+    }
+    const int fcell = (x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz;
+    R rho_w = R(-1);   // lazily computed wall density (UBB, compressible)
+#pragma unroll
+    for (int i = 1; i < Q; ++i) {
+        const int bt = g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK;
+        if (bt == 0) continue;
+        // f_out(x, inv i): where the previous step wrote direction inv(i) of this cell
+        const int j = L::inv(i);
+        const int off = nb.off(PA::template woff<Q>(j, 0), PA::template woff<Q>(j, 1), PA::template woff<Q>(j, 2));
+        R v = Conv<S, R>::ld(src + (long long)PA::template wslot<Q>(j) * g.sq + cell + off);
+        if (bt >= FLAG_UBB0) {
+            const double* uw = a.p.ubb[bt - FLAG_UBB0];
+            R rho = R(1);
+            if (a.p.compressible) {
+                if (rho_w < R(0)) {
+                    R s = 0;
+#pragma unroll
+                    for (int k = 0; k < Q; ++k) {
+                        const int ok = nb.off(PA::template woff<Q>(k, 0), PA::template woff<Q>(k, 1),
+                                              PA::template woff<Q>(k, 2));
+                        s += Conv<S, R>::ld(src + (long long)PA::template wslot<Q>(k) * g.sq + cell + ok);
+                    }
+                    rho_w = R(1) + s;
+                }
+                rho = rho_w;
+            }
+            const R cu = R(L::cx(i)) * R(uw[0]) + R(L::cy(i)) * R(uw[1]) + R(L::cz(i)) * R(uw[2]);
+            v += R(6) * R(L::w(i)) * cu * rho;
+        }
+        f[i] = v;
+    }
+}
+
+template <class S, class R, int Q, int MK, int PAT>
+__global__ void __launch_bounds__(256) k_sweep(const SweepArgs a) {
+    using L = Lat<Q>;
+    using A = Access<PAT>;
+    const Grid& g = a.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.nx || y >= g.ny) return;
+    int fl = 0;
+    if (g.flags != nullptr) {
+        fl = g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz];
+        if (fl & FLAG_TYPE_MASK) return;
+    }
+    NbrOffsets nb;
+    nb.init(g, x, y, z);
+    const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
+    const S* src = static_cast<const S*>(a.src);
+    S* dst = static_cast<S*>(a.dst);
+    R f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
+        f[i] = Conv<S, R>::ld(src + (long long)A::template rslot<Q>(i) * g.sq + cell + off);
+    }
+    if (fl & FLAG_NEAR_WALL) bounce_back<S, R, Q, PAT>(f, a, nb, cell, x, y, z);
+    const R om = collide<R, Q, MK>(f, a.p);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
+        Conv<S, R>::st(dst + (long long)A::template wslot<Q>(i) * g.sq + cell + off, f[i]);
+    }
+    if (a.omega_out != nullptr) a.omega_out[x + g.nx * (y + (long long)g.ny * z)] = (float)om;
+}
+
+// ------------------------------------------------------------------ setter / getter
+struct MacroArgs {
+    Grid g;
+    Physics p;
+    void* pdfs;
+    void* rho;              // R*, element strides rs[3]
+    void* u;                // R*, element strides us[4] (x, y, z, component)
+    long long rs[3];
+    long long us[4];
+};
+
+// Equilibrium initialisation through the write accessor of the previous step
+// (macroscopic_value_kernels.py:29-45); the velocity is shifted by -F/(2 rho_ref) when a force
+// model is present (forcemodels.py:592-593).
+template <class S, class R, int Q, int MK, int PAT>
+__global__ void __launch_bounds__(256) k_set_equilibrium(const MacroArgs a) {
+    using A = Access<PAT>;
+    const Grid& g = a.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.nx || y >= g.ny) return;
+    const R* rp = static_cast<const R*>(a.rho);
+    const R* up = static_cast<const R*>(a.u);
+    const R rho = rp[x * a.rs[0] + y * a.rs[1] + z * a.rs[2]];
+    const long long ub = x * a.us[0] + y * a.us[1] + z * a.us[2];
+    R ux = up[ub], uy = up[ub + a.us[3]], uz = up[ub + 2 * a.us[3]];
+    if (a.p.force_model != FM_NONE) {
+        const R h = R(0.5) / (a.p.compressible ? rho : R(1));
+        ux -= h * R(a.p.force[0]); uy -= h * R(a.p.force[1]); uz -= h * R(a.p.force[2]);
+    }
+    R f[Q];
+    equilibrium<Q, R, MK>(f, rho, ux, uy, uz, a.p);
+    NbrOffsets nb;
+    nb.init(g, x, y, z);
+    const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
+    S* dst = static_cast<S*>(a.pdfs);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
+        Conv<S, R>::st(dst + (long long)A::template wslot<Q>(i) * g.sq + cell + off, f[i]);
+    }
+}
+
+// Density and velocity of the values the previous step wrote (macroscopic_value_kernels.py:48-61,
+// conservedquantitycomputation.py:274-374).
+template <class S, class R, int Q, int PAT>
+__global__ void __launch_bounds__(256) k_get_macroscopic(const MacroArgs a) {
+    using A = Access<PAT>;
+    const Grid& g = a.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.nx || y >= g.ny) return;
+    NbrOffsets nb;
+    nb.init(g, x, y, z);
+    const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
+    const S* src = static_cast<const S*>(a.pdfs);
+    R f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
+        f[i] = Conv<S, R>::ld(src + (long long)A::template wslot<Q>(i) * g.sq + cell + off);
+    }
+    Macro<Q, R> m = conserved<Q, R>(f, a.p, false);
+    if (a.p.force_model != FM_NONE) {
+        const R h = R(0.5) / m.rho_ref;
+        m.ux += h * R(a.p.force[0]); m.uy += h * R(a.p.force[1]); m.uz += h * R(a.p.force[2]);
+    }
+    R* rp = static_cast<R*>(a.rho);
+    R* up = static_cast<R*>(a.u);
+    if (rp) rp[x * a.rs[0] + y * a.rs[1] + z * a.rs[2]] = m.rho;
+    if (up) {
+        const long long ub = x * a.us[0] + y * a.us[1] + z * a.us[2];
+        up[ub] = m.ux; up[ub + a.us[3]] = m.uy; up[ub + 2 * a.us[3]] = m.uz;
+    }
+}
+
+// ------------------------------------------------------------------ FP64 conserved sums
+// Per-block partial sums of mass, momentum (rho_ref * u, force-shifted) and kinetic energy over
+// fluid cells; k_reduce_finish adds the partials in a fixed order (deterministic).
+constexpr int RED_THREADS = 256;
+
+template <class S, int Q, int PAT>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_partial(const MacroArgs a, double* partial) {
+    using A = Access<PAT>;
+    const Grid& g = a.g;
+    double acc[5] = {0, 0, 0, 0, 0};
+    const long long ncell = (long long)g.nx * g.ny * g.nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(c % g.nx);
+        const int y = (int)((c / g.nx) % g.ny);
+        const int z = (int)(c / ((long long)g.nx * g.ny));
+        if (g.flags != nullptr && (g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz] & FLAG_TYPE_MASK)) continue;
+        NbrOffsets nb;
+        nb.init(g, x, y, z);
+        const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
+        const S* src = static_cast<const S*>(a.pdfs);
+        double f[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
+            f[i] = Conv<S, double>::ld(src + (long long)A::template wslot<Q>(i) * g.sq + cell + off);
+        }
+        Macro<Q, double> m = conserved<Q, double>(f, a.p, false);
+        if (a.p.force_model != FM_NONE) {
+            const double h = 0.5 / m.rho_ref;
+            m.ux += h * a.p.force[0]; m.uy += h * a.p.force[1]; m.uz += h * a.p.force[2];
+        }
+        acc[0] += m.rho;
+        acc[1] += m.rho_ref * m.ux;
+        acc[2] += m.rho_ref * m.uy;
+        acc[3] += m.rho_ref * m.uz;
+        acc[4] += 0.5 * m.rho * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
+    }
+    __shared__ double sh[5][RED_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        double v = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double v = 0;
+        for (int w = 0; w < RED_THREADS / 32; ++w) v += sh[threadIdx.x][w];
+        partial[blockIdx.x * 5 + threadIdx.x] = v;
+    }
+}
+
+static __global__ void k_reduce_finish(const double* partial, int nblocks, double* out) {
+    const int k = threadIdx.x;
+    if (k < 5) {
+        double v = 0;
+        for (int b = 0; b < nblocks; ++b) v += partial[b * 5 + k];
+        out[k] = v;
+    }
+}
+
+}  // namespace lbm

@@ -1,0 +1,6 @@
+// Kernel instantiations: D3Q27, MRT collision, FP64/FP32 storage, pull and AA.
+#include "lbm_dispatch.h"
+
+namespace lbm {
+LBM_DEFINE_FAMILY_REDUCED(q27_mrt, 27, MK_MRT)
+}  // namespace lbm

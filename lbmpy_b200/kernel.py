@@ -1,0 +1,188 @@
+"""The callable returned by ``create_lb_function``: launches the fused sm_100a sweep.
+
+lbmpy's ``create_lb_function`` returns a pystencils ``KernelWrapper`` that is called with the
+fields by name and free symbols as keyword arguments (``lbstep.py:269,280``).  ``LbKernel`` keeps
+that calling convention: ``kernel(src=pdfs, dst=tmp, omega=1.8)`` for two-field pull,
+``kernel(src=pdfs)`` for in-place AA / EsoTwist.  Extra keyword arguments beyond lbmpy's:
+``flags`` (uint8 cell flags), ``ubb_velocities`` (wall velocities of UBB numbers 0..3),
+``periodicity`` (overrides ``builtin_periodicity``), ``omega_out`` (float32 field receiving the
+effective shear rate) and ``stream`` (a ``torch.cuda.Stream``).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, Optional, Sequence
+
+import torch
+
+from . import _native as N
+from .enums import Timestep
+from .fields import check_pdf_tensor
+from . import forcemodels
+
+_METHOD = {"srt": N.METHOD_SRT, "trt": N.METHOD_TRT, "mrt": N.METHOD_MRT, "cumulant": N.METHOD_CUMULANT}
+_PATTERN = {"pull": N.PATTERN_PULL, "aa": N.PATTERN_AA, "esotwist": N.PATTERN_ESOTWIST}
+_DT = {"float64": N.DTYPE_F64, "float32": N.DTYPE_F32, "float16": N.DTYPE_F16, "bfloat16": N.DTYPE_BF16}
+
+
+def _evaluate(value, params: Dict):
+    if isinstance(value, (int, float)):
+        return float(value)
+    try:
+        return float(value)
+    except (TypeError, ValueError):
+        pass
+    import sympy as sp
+    expr = sp.sympify(value)
+    subs = {}
+    for s in expr.free_symbols:
+        if s.name not in params:
+            raise ValueError(f"kernel parameter {s.name!r} has no value: pass {s.name}=... when calling the kernel")
+        subs[s] = params[s.name]
+    return float(expr.subs(subs))
+
+
+def free_parameters(update_rule) -> set:
+    names = set()
+    for r in update_rule.method.relaxation_rates:
+        if not isinstance(r, (int, float)):
+            try:
+                float(r)
+            except (TypeError, ValueError):
+                import sympy as sp
+                names |= {s.name for s in sp.sympify(r).free_symbols}
+    return names
+
+
+def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None) -> N.LbmPlanDesc:
+    """Resolves an update rule plus parameter values into the C plan descriptor."""
+    rule = update_rule.collision_rule
+    m = rule.method
+    d = N.LbmPlanDesc()
+    d.stencil = m.stencil.Q
+    d.method = _METHOD[m.kind]
+    d.store_dtype = _DT[update_rule.storage_dtype]
+    d.pattern = _PATTERN[update_rule.streaming_pattern]
+    d.compressible = int(bool(m.compressible))
+    d.continuous_equilibrium = int(bool(m.continuous_equilibrium))
+    rates = [_evaluate(r, params) for r in m.relaxation_rates]
+    if m.kind in ("srt", "trt"):
+        from . import methods as M
+        monos = M.default_monomials(m.stencil.name)
+        even = next(r for r, e in zip(rates, monos) if sum(e) % 2 == 0 and sum(e) > 0)
+        odd = next(r for r, e in zip(rates, monos) if sum(e) % 2 == 1)
+        native_rates = [even, odd]
+    else:
+        native_rates = rates
+    for k, r in enumerate(native_rates):
+        d.rates[k] = r
+    fm = m.force_model
+    if fm is not None:
+        d.force_model = fm.native_id
+        f = [_evaluate(v, params) for v in fm.force] + [0.0] * 3
+        for k in range(3):
+            d.force[k] = f[k]
+    d.galilean_correction = int(bool(rule.galilean_correction))
+    shear = _evaluate(m.shear_relaxation_rate, params)
+    d.shear_rate = shear
+    if rule.subgrid_scale_model is not None:
+        d.sgs = N.SGS_SMAGORINSKY
+        d.sgs_constant = float(rule.smagorinsky_constant)
+        mask = 0
+        # every moment whose (numeric) rate equals the shear rate is adapted, as lbmpy substitutes the
+        # shared rate symbol (methods/abstractlbmethod.py:102-131, turbulence_models.py:55-63)
+        for k, r in enumerate(native_rates):
+            if r == shear:
+                mask |= 1 << k
+        d.sgs_mask = mask
+    for u, vel in enumerate((ubb_velocities or [])[:4]):
+        vel = list(vel) + [0.0] * 3
+        for k in range(3):
+            d.ubb_velocity[u][k] = float(vel[k])
+    for k in range(3):
+        d.dims[k] = int(dims[k])
+        d.periodic[k] = int(bool(periodic[k]))
+    return d
+
+
+def _stream_handle(stream) -> Optional[int]:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, torch.cuda.Stream):
+        return stream.cuda_stream
+    return int(stream)
+
+
+class LbKernel:
+    def __init__(self, update_rule):
+        self.update_rule = update_rule
+        self.method = update_rule.method
+        self._plans = {}
+        self.parameters = free_parameters(update_rule)
+
+    @property
+    def q(self):
+        return self.method.stencil.Q
+
+    def plan(self, dims, periodic, params=None, ubb_velocities=None) -> N.Plan:
+        desc = build_desc(self.update_rule, dims, periodic, params or {}, ubb_velocities)
+        key = (tuple(dims), tuple(bool(p) for p in periodic), torch.cuda.current_device())
+        p = self._plans.get(key)
+        if p is None:
+            p = N.Plan(desc)
+            self._plans[key] = p
+        elif bytes(p.desc) != bytes(desc):
+            p.update(desc)
+        return p
+
+    def _parity(self):
+        ts = self.update_rule.timestep
+        return 1 if ts == Timestep.ODD else 0
+
+    def __call__(self, **kwargs):
+        ur = self.update_rule
+        src = kwargs.pop(ur.field_name, None)
+        if src is None:
+            src = kwargs.pop("pdfs", None)
+        if src is None:
+            raise ValueError(f"missing PDF field {ur.field_name!r}")
+        inplace = ur.streaming_pattern != "pull"
+        dst = kwargs.pop(ur.temporary_field_name, None)
+        if inplace:
+            dst = src
+        elif dst is None:
+            raise ValueError(f"missing temporary PDF field {ur.temporary_field_name!r} for the pull pattern")
+        flags = kwargs.pop("flags", None)
+        ubb = kwargs.pop("ubb_velocities", None)
+        periodic = kwargs.pop("periodicity", ur.builtin_periodicity)
+        omega_out = kwargs.pop("omega_out", None)
+        stream = kwargs.pop("stream", None)
+        parity = kwargs.pop("parity", None)
+        unknown = set(kwargs) - self.parameters
+        if unknown:
+            raise ValueError(f"unknown kernel arguments {sorted(unknown)}; parameters are {sorted(self.parameters)}")
+        check_pdf_tensor(src, self.q, ur.storage_dtype, ur.field_name)
+        check_pdf_tensor(dst, self.q, ur.storage_dtype, ur.temporary_field_name)
+        if dst.shape != src.shape or dst.stride() != src.stride():
+            raise ValueError("src and dst must have the same shape and strides")
+        dims = [s - 2 for s in src.shape[:3]]
+        if flags is not None:
+            if flags.dtype != torch.uint8 or tuple(flags.shape) != tuple(src.shape[:3]) or not flags.is_cuda:
+                raise ValueError("flags must be a CUDA uint8 tensor over the ghost-inclusive domain")
+            if flags.stride() != (1, flags.shape[0], flags.shape[0] * flags.shape[1]):
+                raise ValueError("flags must be contiguous with x fastest")
+        if omega_out is not None:
+            if omega_out.dtype != torch.float32 or omega_out.numel() != dims[0] * dims[1] * dims[2]:
+                raise ValueError("omega_out must be a float32 tensor with one entry per interior cell")
+        plan = self.plan(dims, periodic, kwargs, ubb)
+        strides = N.i64_array(src.stride())
+        par = self._parity() if parity is None else int(parity)
+        N.check(N.lib().lbm_sweep(plan.handle, ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr()),
+                                  strides, ctypes.c_void_p(flags.data_ptr() if flags is not None else None),
+                                  par, ctypes.c_void_p(omega_out.data_ptr() if omega_out is not None else None),
+                                  ctypes.c_void_p(_stream_handle(stream))), "lbm_sweep")
+
+    def __repr__(self):
+        ur = self.update_rule
+        return (f"LbKernel({self.method!r}, pattern={ur.streaming_pattern}, timestep={ur.timestep!s}, "
+                f"storage={ur.storage_dtype})")

@@ -1,0 +1,259 @@
+"""ctypes front end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loaded by tests/, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` leg of ``bench.py`` as
+the checker; the product never imports it.  Arrays follow lbmpy's convention: shape
+``(X+2, Y+2, Z+2, Q)`` (ghost layer included) with the fzyx memory layout (x fastest, PDF index
+slowest), i.e. ``arr[x, y, z, q]`` with numpy strides ``(8, 8*(X+2), ..., ...)``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from fractions import Fraction
+
+import numpy as np
+import sympy as sp
+
+from . import oracle_spec as spec
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+QMAX, TMAX = 27, 40
+PATTERNS = {"pull": 0, "push": 1, "aa": 2, "esotwist": 3}
+
+
+class OmMethod(ctypes.Structure):
+    _fields_ = [
+        ("D", ctypes.c_int), ("Q", ctypes.c_int),
+        ("c", (ctypes.c_int * 3) * QMAX),
+        ("inv", ctypes.c_int * QMAX),
+        ("w", ctypes.c_double * QMAX),
+        ("kind", ctypes.c_int),
+        ("compressible", ctypes.c_int), ("zero_centered", ctypes.c_int),
+        ("delta_eq", ctypes.c_int), ("eq_order", ctypes.c_int),
+        ("nterms", ctypes.c_int * QMAX),
+        ("texp", ((ctypes.c_int * 3) * TMAX) * QMAX),
+        ("tcoef", (ctypes.c_double * TMAX) * QMAX),
+        ("M", (ctypes.c_double * QMAX) * QMAX),
+        ("Minv", (ctypes.c_double * QMAX) * QMAX),
+        ("rate", ctypes.c_double * QMAX),
+        ("force_model", ctypes.c_int),
+        ("F", ctypes.c_double * 3),
+        ("galilean", ctypes.c_int),
+        ("sgs", ctypes.c_int),
+        ("sgs_c", ctypes.c_double),
+        ("shear_rate", ctypes.c_double),
+    ]
+
+
+class OmGrid(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int * 3), ("g", ctypes.c_int * 3), ("s", ctypes.c_int64 * 4)]
+
+
+def build():
+    """Compile the oracle library in place (make in this directory)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liblbm_oracle.so")
+        if not os.path.exists(path):
+            build()
+        _LIB = ctypes.CDLL(path)
+        dp = ctypes.POINTER(ctypes.c_double)
+        _LIB.om_sizeof_method.restype = ctypes.c_int
+        assert _LIB.om_sizeof_method() == ctypes.sizeof(OmMethod), "oracle struct layout mismatch"
+        _LIB.om_run.restype = ctypes.c_int
+    return _LIB
+
+
+def _exact_inverse(rows):
+    n = len(rows)
+    a = [[Fraction(v) for v in r] + [Fraction(int(i == j)) for j in range(n)] for i, r in enumerate(rows)]
+    for col in range(n):
+        piv = next(r for r in range(col, n) if a[r][col] != 0)
+        a[col], a[piv] = a[piv], a[col]
+        p = a[col][col]
+        a[col] = [v / p for v in a[col]]
+        for r in range(n):
+            if r != col and a[r][col] != 0:
+                fct = a[r][col]
+                a[r] = [v - fct * pv for v, pv in zip(a[r], a[col])]
+    return [row[n:] for row in a]
+
+
+class Oracle:
+    """A resolved lbmpy method on the CPU oracle."""
+
+    def __init__(self, method: spec.OracleMethod):
+        self.spec = method
+        m = OmMethod()
+        dirs = method.dirs
+        D, Q = method.D, method.Q
+        m.D, m.Q = D, Q
+        for i, d in enumerate(dirs):
+            d3 = tuple(d) + (0,) * (3 - D)
+            for k in range(3):
+                m.c[i][k] = d3[k]
+            m.inv[i] = dirs.index(tuple(-v for v in d))
+            m.w[i] = float(method.weights[i])
+        m.kind = method.kind
+        m.compressible = int(method.compressible)
+        m.zero_centered = int(method.zero_centered)
+        m.delta_eq = int(method.delta_equilibrium)
+        m.eq_order = method.equilibrium_order
+        for k, mom in enumerate(method.moments):
+            terms = spec.poly_terms(mom)
+            assert len(terms) <= TMAX
+            m.nterms[k] = len(terms)
+            for t, (coef, e) in enumerate(terms):
+                m.tcoef[k][t] = float(coef)
+                for j in range(3):
+                    m.texp[k][t][j] = e[j]
+            m.rate[k] = method.rates[k]
+        if method.kind == spec.KIND_MOMENT:
+            M = spec.moment_matrix(method.moments, dirs)
+        else:
+            monos = [(a, b, c) for a in range(3) for b in range(3) for c in range(3)]
+            M = []
+            for mom in method.moments:
+                row = [Fraction(0)] * 27
+                for coef, e in spec.poly_terms(mom):
+                    row[monos.index(e)] += coef
+                M.append(row)
+        Minv = _exact_inverse(M)
+        for k in range(Q):
+            for i in range(Q):
+                m.M[k][i] = float(M[k][i])
+                m.Minv[k][i] = float(Minv[k][i])
+        m.force_model = method.force_model
+        for k in range(3):
+            m.F[k] = method.force[k]
+        m.galilean = int(method.galilean_correction)
+        m.sgs = method.sgs
+        m.sgs_c = method.sgs_constant
+        m.shear_rate = method.shear_rate
+        self._m = m
+        self.M = np.array([[float(v) for v in r] for r in M])
+        self.Minv = np.array([[float(v) for v in r] for r in Minv])
+
+    # -- helpers -------------------------------------------------------------------------------
+    @property
+    def Q(self):
+        return self.spec.Q
+
+    @property
+    def D(self):
+        return self.spec.D
+
+    def new_field(self, shape):
+        """Zeroed PDF array for an interior domain `shape` in lbmpy's fzyx layout."""
+        shape = tuple(shape) + (1,) * (3 - len(shape))
+        ext = [s + 2 for s in shape[:self.D]] + [1] * (3 - self.D)
+        buf = np.zeros((self.Q, ext[2], ext[1], ext[0]), dtype=np.float64)
+        return buf.transpose(3, 2, 1, 0)
+
+    def _grid(self, arr):
+        g = OmGrid()
+        ext = arr.shape[:3]
+        for d in range(3):
+            gl = 1 if d < self.D else 0
+            g.g[d] = gl
+            g.n[d] = ext[d] - 2 * gl
+        for d in range(4):
+            g.s[d] = arr.strides[d] // 8
+        return g
+
+    @staticmethod
+    def _ptr(a):
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+    # -- kernels -------------------------------------------------------------------------------
+    def collide(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.zeros_like(f)
+        om = ctypes.c_double(0.0)
+        lib().om_collide(ctypes.byref(self._m), self._ptr(f), self._ptr(out), ctypes.byref(om))
+        return out
+
+    def equilibrium(self, rho, u):
+        u3 = np.zeros(3)
+        u3[:len(u)] = u
+        out = np.zeros(self.Q)
+        lib().om_equilibrium(ctypes.byref(self._m), ctypes.c_double(rho), self._ptr(u3), self._ptr(out))
+        return out
+
+    def set_equilibrium(self, f, rho, u, pattern="pull", prev_parity=0):
+        """rho: interior shape; u: interior shape + (D,)."""
+        g = self._grid(f)
+        n = (g.n[0], g.n[1], g.n[2])
+        rho_c = np.ascontiguousarray(np.broadcast_to(rho, n[:self.D]).reshape(n).transpose(2, 1, 0), np.float64)
+        u3 = np.zeros((3,) + n[::-1])
+        uu = np.asarray(u, np.float64).reshape(n + (self.D,))
+        for d in range(self.D):
+            u3[d] = uu[..., d].transpose(2, 1, 0)
+        lib().om_set_equilibrium(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], prev_parity,
+                                 self._ptr(rho_c), self._ptr(u3), self._ptr(f))
+
+    def get_macroscopic(self, f, pattern="pull", prev_parity=0):
+        g = self._grid(f)
+        n = (g.n[0], g.n[1], g.n[2])
+        rho = np.zeros(n[::-1])
+        u3 = np.zeros((3,) + n[::-1])
+        lib().om_get_macroscopic(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], prev_parity,
+                                 self._ptr(f), self._ptr(rho), self._ptr(u3))
+        rho = rho.transpose(2, 1, 0)[(slice(None),) * self.D + (0,) * (3 - self.D)]
+        u = np.stack([u3[d].transpose(2, 1, 0) for d in range(self.D)], axis=-1)
+        u = u[(slice(None),) * self.D + (0,) * (3 - self.D)]
+        return rho, u
+
+    def run(self, f, steps, pattern="pull", parity=0, periodic=(True, True, True), flags=None,
+            ubb_velocity=(0.0, 0.0, 0.0), tmp=None):
+        """Runs `steps` time steps.  Returns (field holding the result, new parity)."""
+        g = self._grid(f)
+        per = (ctypes.c_int * 3)(*[int(p) for p in periodic])
+        par = ctypes.c_int(parity)
+        ub = np.array(list(ubb_velocity) + [0.0] * (3 - len(ubb_velocity)), np.float64)
+        fl = None
+        if flags is not None:
+            fl = np.ascontiguousarray(flags.transpose(2, 1, 0) if flags.ndim == 3 else flags.T, np.uint8)
+        if pattern in ("pull", "push"):
+            if tmp is None:
+                tmp = np.zeros_like(f)
+                tmp = self.new_field(tuple(s - 2 for s in f.shape[:self.D]))
+                tmp[...] = f
+            sw = lib().om_run(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], ctypes.byref(par),
+                              steps, per, fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None
+                              else None, self._ptr(ub), self._ptr(f), self._ptr(tmp))
+            return (tmp if sw else f), par.value
+        lib().om_run(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], ctypes.byref(par), steps, per,
+                     fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None else None,
+                     self._ptr(ub), self._ptr(f), self._ptr(f))
+        return f, par.value
+
+    def periodic_sync(self, f, pattern="pull", prev_parity=0, periodic=(True, True, True)):
+        """Moves values the previous step wrote into ghost cells to their periodic images and
+        refreshes the periodic ghost layers (the oracle's communication step)."""
+        g = self._grid(f)
+        per = (ctypes.c_int * 3)(*[int(p) for p in periodic])
+        lib().om_periodic_sync(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], prev_parity, per,
+                               self._ptr(f))
+
+    def reduce(self, f, pattern="pull", prev_parity=0, flags=None):
+        g = self._grid(f)
+        out = np.zeros(5)
+        fl = None
+        if flags is not None:
+            fl = np.ascontiguousarray(flags.transpose(2, 1, 0) if flags.ndim == 3 else flags.T, np.uint8)
+        lib().om_reduce(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], prev_parity, self._ptr(f),
+                        fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None else None,
+                        self._ptr(out))
+        return out
+
+
+def make(stencil, method, **kw) -> Oracle:
+    return Oracle(spec.resolve(stencil, method, **kw))
