@@ -97,15 +97,15 @@ int lbm_run(const LbmPlan* plan, void* a, void* b, const int64_t strides[4], con
 
 /* Equilibrium initialisation through the write accessor of the previous step
  * (macroscopic_value_kernels.py:29-45, compile_macroscopic_values_setter :170-242).
- * rho / u element type: double for F64 storage, float otherwise.  rho_strides: x, y, z;
- * u_strides: x, y, z, component (elements). */
+ * rho / u element type: double (for every storage type; the equilibrium is evaluated in FP64).
+ * rho_strides: x, y, z; u_strides: x, y, z, component (elements). */
 int lbm_set_equilibrium(const LbmPlan* plan, void* pdfs, const int64_t strides[4], const void* rho,
                         const int64_t rho_strides[3], const void* u, const int64_t u_strides[4],
                         int prev_parity, void* stream);
 
 /* Density and velocity from the values the previous step wrote
  * (macroscopic_value_kernels.py:48-61, compile_macroscopic_values_getter :88-167).
- * rho or u may be NULL. */
+ * rho / u element type: double for F64 storage, float otherwise; either may be NULL. */
 int lbm_get_macroscopic(const LbmPlan* plan, const void* pdfs, const int64_t strides[4], void* rho,
                         const int64_t rho_strides[3], void* u, const int64_t u_strides[4],
                         int prev_parity, void* stream);

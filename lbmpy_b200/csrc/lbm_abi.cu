@@ -79,6 +79,8 @@ int check_strides(const LbmPlan* p, const int64_t s[4]) {
                     (long long)ey, (long long)ez);
     if ((ex - 1) + (ey - 1) * s[1] + (ez - 1) * s[2] >= (int64_t(1) << 31))
         return fail(LBM_E_INVALID, "one PDF slot plane must hold fewer than 2^31 elements");
+    if (s[3] * (int64_t)p->q >= (int64_t(1) << 32))
+        return fail(LBM_E_INVALID, "the PDF field must span fewer than 2^32 elements (32-bit indexing)");
     return LBM_OK;
 }
 
@@ -89,7 +91,7 @@ Grid make_grid(const LbmPlan* p, const int64_t s[4], const uint8_t* flags) {
     g.nz = p->desc.dims[2];
     g.sy = (int)s[1];
     g.sz = (int)s[2];
-    g.sq = s[3];
+    g.sq = (unsigned)s[3];
     g.periodic = (p->desc.periodic[0] ? 1 : 0) | (p->desc.periodic[1] ? 2 : 0) | (p->desc.periodic[2] ? 4 : 0);
     g.flags = flags;
     g.fsy = g.nx + 2;
@@ -120,6 +122,7 @@ SweepLauncher sweep_launcher(const LbmPlan* p, int pat) {
     if (p->q == 27 && p->mk == MK_POP) return sweep_q27_pop(p->store, pat);
     if (p->q == 27 && p->mk == MK_MRT) return sweep_q27_mrt(p->store, pat);
     if (p->q == 27 && p->mk == MK_CUM) return sweep_q27_cum(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM1) return sweep_q27_cum1(p->store, pat);
     return nullptr;
 }
 
@@ -128,7 +131,7 @@ MacroLauncher set_eq_launcher(const LbmPlan* p, int pat) {
     if (p->q == 19 && p->mk == MK_MRT) return set_eq_q19_mrt(p->store, pat);
     if (p->q == 27 && p->mk == MK_POP) return set_eq_q27_pop(p->store, pat);
     if (p->q == 27 && p->mk == MK_MRT) return set_eq_q27_mrt(p->store, pat);
-    if (p->q == 27 && p->mk == MK_CUM) return set_eq_q27_cum(p->store, pat);
+    if (p->q == 27 && (p->mk == MK_CUM || p->mk == MK_CUM1)) return set_eq_q27_cum(p->store, pat);
     return nullptr;
 }
 
@@ -238,6 +241,16 @@ int fill_physics(LbmPlan* p, const LbmPlanDesc* d) {
     return LBM_OK;
 }
 
+// Every cumulant group of order >= 3 (canonical indices 10..26) has rate 1 and no SGS adaptation:
+// the specialised cumulant sweep applies.
+bool cumulant_high_orders_relax_to_equilibrium(const LbmPlanDesc* d) {
+    for (int k = 10; k < 27; ++k) {
+        if (d->rates[k] != 1.0) return false;
+        if (d->sgs != LBM_SGS_NONE && ((d->sgs_mask >> k) & 1u)) return false;
+    }
+    return true;
+}
+
 int validate_desc(const LbmPlanDesc* d) {
     if (d->stencil != 19 && d->stencil != 27) return fail(LBM_E_UNSUPPORTED, "stencil must be D3Q19 or D3Q27");
     if (d->method < 0 || d->method > 3) return fail(LBM_E_INVALID, "unknown method %d", d->method);
@@ -288,6 +301,7 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
     if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaGetDevice"); }
     p->q = desc->stencil;
     p->mk = desc->method == LBM_METHOD_MRT ? MK_MRT : (desc->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
+    if (p->mk == MK_CUM && cumulant_high_orders_relax_to_equilibrium(desc)) p->mk = MK_CUM1;
     p->store = desc->store_dtype;
     fill_physics(p, desc);
     int sms = 148;
@@ -314,6 +328,8 @@ int lbm_plan_update(LbmPlan* p, const LbmPlanDesc* desc) {
     int rc = validate_desc(desc);
     if (rc) return rc;
     p->desc = *desc;
+    p->mk = desc->method == LBM_METHOD_MRT ? MK_MRT : (desc->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
+    if (p->mk == MK_CUM && cumulant_high_orders_relax_to_equilibrium(desc)) p->mk = MK_CUM1;
     fill_physics(p, desc);
     return LBM_OK;
 }
@@ -325,8 +341,8 @@ int lbm_plan_destroy(LbmPlan* p) {
     return LBM_OK;
 }
 
-int lbm_sweep(const LbmPlan* p, const void* src, void* dst, const int64_t strides[4], const uint8_t* flags,
-              int parity, float* omega_out, void* stream) {
+static int validate_sweep(const LbmPlan* p, const void* src, const void* dst, const int64_t strides[4],
+                          const uint8_t* flags, const float* omega_out) {
     if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
     int rc;
     if ((rc = check_device(p))) return rc;
@@ -338,10 +354,15 @@ int lbm_sweep(const LbmPlan* p, const void* src, void* dst, const int64_t stride
     const bool inplace = p->desc.pattern != LBM_PATTERN_PULL;
     if (inplace && src != dst) return fail(LBM_E_INVALID, "in-place streaming patterns need src == dst");
     if (!inplace && src == dst) return fail(LBM_E_INVALID, "the pull pattern needs two distinct fields");
-    if (parity != 0 && parity != 1) return fail(LBM_E_INVALID, "parity must be 0 (EVEN) or 1 (ODD)");
+    return LBM_OK;
+}
+
+// Launch without re-validating (arguments checked by the caller).
+static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, const int64_t strides[4],
+                                const uint8_t* flags, int parity, float* omega_out, cudaStream_t stream) {
     const int pat = pattern_kind(p, parity);
     SweepLauncher L = sweep_launcher(p, pat);
-    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no kernel for this pattern");
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no kernel for this storage type / pattern");
     SweepArgs a;
     a.g = make_grid(p, strides, flags);
     a.p = p->phys;
@@ -350,22 +371,33 @@ int lbm_sweep(const LbmPlan* p, const void* src, void* dst, const int64_t stride
     a.omega_out = omega_out;
     dim3 grid, block;
     launch_shape(a.g, grid, block);
-    cudaError_t e = L(a, grid, block, static_cast<cudaStream_t>(stream));
+    cudaError_t e = L(a, grid, block, stream);
     if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
     return LBM_OK;
+}
+
+int lbm_sweep(const LbmPlan* p, const void* src, void* dst, const int64_t strides[4], const uint8_t* flags,
+              int parity, float* omega_out, void* stream) {
+    int rc = validate_sweep(p, src, dst, strides, flags, omega_out);
+    if (rc) return rc;
+    if (parity != 0 && parity != 1) return fail(LBM_E_INVALID, "parity must be 0 (EVEN) or 1 (ODD)");
+    return launch_sweep_checked(p, src, dst, strides, flags, parity, omega_out, static_cast<cudaStream_t>(stream));
 }
 
 int lbm_run(const LbmPlan* p, void* a, void* b, const int64_t strides[4], const uint8_t* flags, int first_parity,
             int steps, int* result_in_b, void* stream) {
     if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
     if (steps < 0) return fail(LBM_E_INVALID, "steps must be >= 0");
+    if (first_parity != 0 && first_parity != 1) return fail(LBM_E_INVALID, "parity must be 0 (EVEN) or 1 (ODD)");
     const bool inplace = p->desc.pattern != LBM_PATTERN_PULL;
+    int rc = validate_sweep(p, a, inplace ? a : b, strides, flags, nullptr);
+    if (rc) return rc;
     void* src = a;
     void* dst = inplace ? a : b;
     int parity = first_parity;
     int in_b = 0;
     for (int t = 0; t < steps; ++t) {
-        int rc = lbm_sweep(p, src, dst, strides, flags, parity, nullptr, stream);
+        rc = launch_sweep_checked(p, src, dst, strides, flags, parity, nullptr, static_cast<cudaStream_t>(stream));
         if (rc) return rc;
         if (inplace) parity ^= 1;
         else { void* tmp = src; src = dst; dst = tmp; in_b ^= 1; }

@@ -394,6 +394,150 @@ __device__ __forceinline__ R collide_cum(R (&f)[27], const Physics& p) {
     return p.sgs == 1 ? om_sgs : R(p.rates[4]);
 }
 
+// D3Q27 cumulant when every cumulant of third and higher order relaxes with rate 1 (lbmpy's
+// default for a single relaxation rate, methods/creationfunctions.py:638-652): those post-collision
+// cumulants are zero, so only second-order pre-collision moments are needed.  The post-collision
+// central moments are formed directly as deviations from the central moments of the lattice-weight
+// background, Delta = kappa* - B(u) (B separable: B0 = 1, B1 = -u, B2 = 1/3 + u^2); the inverse
+// transform of Delta gives the zero-centred populations with no O(1/3) cancellation.
+template <class R>
+__device__ __forceinline__ R collide_cum_ho1(R (&f)[27], const Physics& p) {
+    // raw moments of f~ (no shift) on the velocity cube: m[a*9 + b*3 + c]
+    R m[27];
+#pragma unroll
+    for (int i = 0; i < 27; ++i) m[cube<27>(i)] = f[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const int base = a * 9 + b * 3;   // z lines
+            const R fm = m[base], f0 = m[base + 1], fp = m[base + 2];
+            m[base] = fm + f0 + fp; m[base + 1] = fp - fm; m[base + 2] = fp + fm;
+        }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int base = a * 9 + c;       // y lines
+            const R fm = m[base], f0 = m[base + 3], fp = m[base + 6];
+            m[base] = fm + f0 + fp; m[base + 3] = fp - fm; m[base + 6] = fp + fm;
+        }
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int base = b * 3 + c;       // x lines
+            const R fm = m[base], f0 = m[base + 9], fp = m[base + 18];
+            m[base] = fm + f0 + fp; m[base + 9] = fp - fm; m[base + 18] = fp + fm;
+        }
+#define M_(a, b, c) m[(a) * 9 + (b) * 3 + (c)]
+    const R drho = M_(0, 0, 0);
+    const R rho = R(1) + drho, irho = R(1) / rho;
+    const bool cm_force = p.force_model == FM_CENTRAL;
+    R ux = M_(1, 0, 0) * irho, uy = M_(0, 1, 0) * irho, uz = M_(0, 0, 1) * irho;
+    const R hx = R(0.5) * R(p.force[0]), hy = R(0.5) * R(p.force[1]), hz = R(0.5) * R(p.force[2]);
+    if (cm_force) { ux += hx * irho; uy += hy * irho; uz += hz * irho; }
+    const R uxx = ux * ux, uyy = uy * uy, uzz = uz * uz;
+    // second-order central moments of the full PDFs minus rho/3 (diagonal) -- small numbers:
+    // kappa_200 = m~200 - 2 ux m~100 + ux^2 m~000 + (1/3 + ux^2), and rho/3 = 1/3 + drho/3
+    const R third = R(1.0 / 3.0);
+    const R a0 = M_(2, 0, 0) - R(2) * ux * M_(1, 0, 0) + uxx * drho + uxx - drho * third;
+    const R b0 = M_(0, 2, 0) - R(2) * uy * M_(0, 1, 0) + uyy * drho + uyy - drho * third;
+    const R c0 = M_(0, 0, 2) - R(2) * uz * M_(0, 0, 1) + uzz * drho + uzz - drho * third;
+    const R k110 = M_(1, 1, 0) - ux * M_(0, 1, 0) - uy * M_(1, 0, 0) + ux * uy * drho + ux * uy;
+    const R k101 = M_(1, 0, 1) - ux * M_(0, 0, 1) - uz * M_(1, 0, 0) + ux * uz * drho + ux * uz;
+    const R k011 = M_(0, 1, 1) - uy * M_(0, 0, 1) - uz * M_(0, 1, 0) + uy * uz * drho + uy * uz;
+#undef M_
+    R om_sgs = R(0);
+    if (p.sgs == 1) {
+        // Pi_neq from the central moments: raw second moments minus their equilibrium values
+        const R pxx = a0 - ux * R(p.force[0]) * R(cm_force ? 1 : 0);
+        const R pyy = b0 - uy * R(p.force[1]) * R(cm_force ? 1 : 0);
+        const R pzz = c0 - uz * R(p.force[2]) * R(cm_force ? 1 : 0);
+        const R fxy = cm_force ? R(0.5) * (ux * R(p.force[1]) + uy * R(p.force[0])) : R(0);
+        const R fxz = cm_force ? R(0.5) * (ux * R(p.force[2]) + uz * R(p.force[0])) : R(0);
+        const R fyz = cm_force ? R(0.5) * (uy * R(p.force[2]) + uz * R(p.force[1])) : R(0);
+        const R pxy = k110 - fxy, pxz = k101 - fxz, pyz = k011 - fyz;
+        const R s2 = pxx * pxx + pyy * pyy + pzz * pzz + R(2) * (pxy * pxy + pxz * pxz + pyz * pyz);
+        const R pi = sqrt(R(2) * s2) * irho;
+        const R tau0 = R(p.tau0);
+        om_sgs = R(2) / (tau0 + sqrt(R(p.sgs_c18) * pi + tau0 * tau0));
+    }
+    auto rate = [&](int idx) -> R {
+        R r = R(p.rates[idx]);
+        if (p.sgs == 1 && ((p.sgs_mask >> idx) & 1u)) r = om_sgs;
+        return r;
+    };
+    const R w_xy = rate(4), w_xz = rate(5), w_yz = rate(6), w_d1 = rate(7), w_d2 = rate(8), w_b = rate(9);
+    R D1 = (a0 - b0) * (R(1) - w_d1);
+    R D2 = (a0 - c0) * (R(1) - w_d2);
+    R Sd = (a0 + b0 + c0) * (R(1) - w_b);   // (sum of diagonal second cumulants) - rho
+    if (p.galilean) {
+        const R o1 = R(p.rates[7]), o2 = R(p.rates[9]);
+        const R h = R(0.5) * irho;
+        // c_xx = rho/3 + a0: 2cxx - cyy - czz = 2a0 - b0 - c0; cxx + cyy + czz - rho = a0 + b0 + c0
+        const R Dx = -o1 * h * (R(2) * a0 - b0 - c0) - o2 * h * (a0 + b0 + c0);
+        const R Dy = Dx + R(3) * o1 * h * (a0 - b0);
+        const R Dz = Dx + R(3) * o1 * h * (a0 - c0);
+        const R g1 = R(-3) * rho * (R(1) - R(0.5) * o1);
+        const R g2 = R(-3) * rho * (R(1) - R(0.5) * o2);
+        D1 += g1 * (uxx * Dx - uyy * Dy);
+        D2 += g1 * (uxx * Dx - uzz * Dz);
+        Sd += g2 * (uxx * Dx + uyy * Dy + uzz * Dz);
+    }
+    const R a = (Sd + D1 + D2) * third;
+    const R b = a - D1, c = a - D2;
+    const R cxy = k110 * (R(1) - w_xy), cxz = k101 * (R(1) - w_xz), cyz = k011 * (R(1) - w_yz);
+
+    // Delta = kappa* - B(u), kappa* built from the post-collision cumulants (orders >= 3 zero)
+    R d[27];
+#define D_(x, y, z) d[(x) * 9 + (y) * 3 + (z)]
+    const R bx2 = third + uxx, by2 = third + uyy, bz2 = third + uzz;
+    D_(0, 0, 0) = drho;
+    D_(1, 0, 0) = ux + (cm_force ? hx : R(0));
+    D_(0, 1, 0) = uy + (cm_force ? hy : R(0));
+    D_(0, 0, 1) = uz + (cm_force ? hz : R(0));
+    D_(2, 0, 0) = a + drho * third - uxx;
+    D_(0, 2, 0) = b + drho * third - uyy;
+    D_(0, 0, 2) = c + drho * third - uzz;
+    D_(1, 1, 0) = cxy - ux * uy;
+    D_(1, 0, 1) = cxz - ux * uz;
+    D_(0, 1, 1) = cyz - uy * uz;
+    // third order: kappa* = 0, Delta = -B
+    D_(1, 1, 1) = ux * uy * uz;
+    D_(2, 1, 0) = bx2 * uy; D_(2, 0, 1) = bx2 * uz;
+    D_(1, 2, 0) = by2 * ux; D_(0, 2, 1) = by2 * uz;
+    D_(1, 0, 2) = bz2 * ux; D_(0, 1, 2) = bz2 * uy;
+    // fourth order
+    const R t9 = R(1.0 / 9.0);
+    D_(2, 2, 0) = drho * t9 + (a + b) * third + (a * b + R(2) * cxy * cxy) * irho - (uxx + uyy) * third - uxx * uyy;
+    D_(2, 0, 2) = drho * t9 + (a + c) * third + (a * c + R(2) * cxz * cxz) * irho - (uxx + uzz) * third - uxx * uzz;
+    D_(0, 2, 2) = drho * t9 + (b + c) * third + (b * c + R(2) * cyz * cyz) * irho - (uyy + uzz) * third - uyy * uzz;
+    D_(2, 1, 1) = cyz * third + (a * cyz + R(2) * cxy * cxz) * irho - bx2 * uy * uz;
+    D_(1, 2, 1) = cxz * third + (b * cxz + R(2) * cxy * cyz) * irho - by2 * ux * uz;
+    D_(1, 1, 2) = cxy * third + (c * cxy + R(2) * cxz * cyz) * irho - bz2 * ux * uy;
+    // fifth order: kappa* = 0
+    D_(2, 2, 1) = bx2 * by2 * uz;
+    D_(2, 1, 2) = bx2 * bz2 * uy;
+    D_(1, 2, 2) = by2 * bz2 * ux;
+    // sixth order
+    {
+        const R i2 = irho * irho;
+        const R ss = cxy * cxy + cxz * cxz + cyz * cyz;
+        D_(2, 2, 2) = drho * (R(1.0 / 27.0)) + (a + b + c) * t9 + (a * b + b * c + a * c) * third * irho +
+                      a * b * c * i2 + R(2.0 / 3.0) * ss * irho +
+                      R(2) * (a * cyz * cyz + b * cxz * cxz + c * cxy * cxy) * i2 + R(8) * cxy * cxz * cyz * i2 -
+                      (uxx + uyy + uzz) * t9 - (uxx * uyy + uxx * uzz + uyy * uzz) * third - uxx * uyy * uzz;
+    }
+#undef D_
+    chimera_backward(d, ux, 9, 3, 1);
+    chimera_backward(d, uy, 3, 9, 1);
+    chimera_backward(d, uz, 1, 9, 3);
+#pragma unroll
+    for (int i = 0; i < 27; ++i) f[i] = d[cube<27>(i)];
+    return p.sgs == 1 ? om_sgs : R(p.rates[4]);
+}
+
 // ------------------------------------------------------------------ equilibria (setter)
 // Zero-centred equilibrium populations of the method at (rho, u) (macroscopic_value_kernels.py:29-45).
 template <int Q, class R, int MK>

@@ -46,6 +46,8 @@ MacroLauncher pick_set_eq_pattern(int pat) {
 }
 
 // Instantiates the sweep and setter families of one (Q, method) pair in one translation unit.
+// The setter always evaluates the equilibrium in FP64 from FP64 density / velocity fields, so
+// that the density deviation rho - 1 keeps its digits before the PDFs are rounded to storage.
 #define LBM_DEFINE_FAMILY(NAME, Q, MK)                                                          \
     SweepLauncher sweep_##NAME(int store, int pat) {                                            \
         switch (store) {                                                                        \
@@ -59,9 +61,9 @@ MacroLauncher pick_set_eq_pattern(int pat) {
     MacroLauncher set_eq_##NAME(int store, int pat) {                                           \
         switch (store) {                                                                        \
             case ST_F64: return pick_set_eq_pattern<double, double, Q, MK>(pat);                 \
-            case ST_F32: return pick_set_eq_pattern<float, float, Q, MK>(pat);                   \
-            case ST_F16: return pick_set_eq_pattern<__half, float, Q, MK>(pat);                  \
-            case ST_BF16: return pick_set_eq_pattern<__nv_bfloat16, float, Q, MK>(pat);         \
+            case ST_F32: return pick_set_eq_pattern<float, double, Q, MK>(pat);                   \
+            case ST_F16: return pick_set_eq_pattern<__half, double, Q, MK>(pat);                  \
+            case ST_BF16: return pick_set_eq_pattern<__nv_bfloat16, double, Q, MK>(pat);         \
         }                                                                                       \
         return nullptr;                                                                         \
     }
@@ -94,7 +96,7 @@ MacroLauncher pick_set_eq_pattern(int pat) {
     }                                                                                           \
     MacroLauncher set_eq_##NAME(int store, int pat) {                                           \
         if (store == ST_F64) return NAME##_set_pat<double, double>(pat);                        \
-        if (store == ST_F32) return NAME##_set_pat<float, float>(pat);                          \
+        if (store == ST_F32) return NAME##_set_pat<float, double>(pat);                          \
         return nullptr;                                                                         \
     }
 
@@ -107,5 +109,6 @@ LBM_DECLARE_FAMILY(q19_mrt)
 LBM_DECLARE_FAMILY(q27_pop)
 LBM_DECLARE_FAMILY(q27_mrt)
 LBM_DECLARE_FAMILY(q27_cum)
+LBM_DECLARE_FAMILY(q27_cum1)
 
 }  // namespace lbm

@@ -56,8 +56,12 @@ template <class R, int Q, int MK>
 __device__ __forceinline__ R collide(R (&f)[Q], const Physics& p) {
     if constexpr (MK == MK_POP) return collide_pop<Q, R>(f, p);
     else if constexpr (MK == MK_MRT) return collide_mrt<Q, R>(f, p);
+    else if constexpr (MK == MK_CUM1) return collide_cum_ho1<R>(f, p);
     else return collide_cum<R>(f, p);
 }
+
+// Element index of (slot, cell + offset) relative to the field base; 32-bit (host-checked).
+__device__ __forceinline__ unsigned eidx(unsigned slot_off, int cell_off) { return slot_off + (unsigned)cell_off; }
 
 // Fused bounce-back for a fluid cell next to a boundary: replaces the pulled value of every
 // direction whose source cell x - c_i is a wall.
@@ -83,7 +87,7 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
         // f_out(x, inv i): where the previous step wrote direction inv(i) of this cell
         const int j = L::inv(i);
         const int off = nb.off(PA::template woff<Q>(j, 0), PA::template woff<Q>(j, 1), PA::template woff<Q>(j, 2));
-        R v = Conv<S, R>::ld(src + (long long)PA::template wslot<Q>(j) * g.sq + cell + off);
+        R v = Conv<S, R>::ld(src + eidx(PA::template wslot<Q>(j) * g.sq, cell + off));
         if (bt >= FLAG_UBB0) {
             const double* uw = a.p.ubb[bt - FLAG_UBB0];
             R rho = R(1);
@@ -94,7 +98,7 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
                     for (int k = 0; k < Q; ++k) {
                         const int ok = nb.off(PA::template woff<Q>(k, 0), PA::template woff<Q>(k, 1),
                                               PA::template woff<Q>(k, 2));
-                        s += Conv<S, R>::ld(src + (long long)PA::template wslot<Q>(k) * g.sq + cell + ok);
+                        s += Conv<S, R>::ld(src + eidx(PA::template wslot<Q>(k) * g.sq, cell + ok));
                     }
                     rho_w = R(1) + s;
                 }
@@ -130,14 +134,14 @@ __global__ void __launch_bounds__(256) k_sweep(const SweepArgs a) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
-        f[i] = Conv<S, R>::ld(src + (long long)A::template rslot<Q>(i) * g.sq + cell + off);
+        f[i] = Conv<S, R>::ld(src + eidx(A::template rslot<Q>(i) * g.sq, cell + off));
     }
     if (fl & FLAG_NEAR_WALL) bounce_back<S, R, Q, PAT>(f, a, nb, cell, x, y, z);
     const R om = collide<R, Q, MK>(f, a.p);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
-        Conv<S, R>::st(dst + (long long)A::template wslot<Q>(i) * g.sq + cell + off, f[i]);
+        Conv<S, R>::st(dst + eidx(A::template wslot<Q>(i) * g.sq, cell + off), f[i]);
     }
     if (a.omega_out != nullptr) a.omega_out[x + g.nx * (y + (long long)g.ny * z)] = (float)om;
 }
@@ -182,7 +186,7 @@ __global__ void __launch_bounds__(256) k_set_equilibrium(const MacroArgs a) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
-        Conv<S, R>::st(dst + (long long)A::template wslot<Q>(i) * g.sq + cell + off, f[i]);
+        Conv<S, R>::st(dst + eidx(A::template wslot<Q>(i) * g.sq, cell + off), f[i]);
     }
 }
 
@@ -204,7 +208,7 @@ __global__ void __launch_bounds__(256) k_get_macroscopic(const MacroArgs a) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
-        f[i] = Conv<S, R>::ld(src + (long long)A::template wslot<Q>(i) * g.sq + cell + off);
+        f[i] = Conv<S, R>::ld(src + eidx(A::template wslot<Q>(i) * g.sq, cell + off));
     }
     Macro<Q, R> m = conserved<Q, R>(f, a.p, false);
     if (a.p.force_model != FM_NONE) {
@@ -245,7 +249,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_partial(const MacroArgs 
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
-            f[i] = Conv<S, double>::ld(src + (long long)A::template wslot<Q>(i) * g.sq + cell + off);
+            f[i] = Conv<S, double>::ld(src + eidx(A::template wslot<Q>(i) * g.sq, cell + off));
         }
         Macro<Q, double> m = conserved<Q, double>(f, a.p, false);
         if (a.p.force_model != FM_NONE) {

@@ -25,7 +25,7 @@ _PATTERN = {"pull": N.PATTERN_PULL, "aa": N.PATTERN_AA, "esotwist": N.PATTERN_ES
 _DT = {"float64": N.DTYPE_F64, "float32": N.DTYPE_F32, "float16": N.DTYPE_F16, "bfloat16": N.DTYPE_BF16}
 
 
-def _evaluate(value, params: Dict):
+def _evaluate(value, params: Dict, placeholder=None):
     if isinstance(value, (int, float)):
         return float(value)
     try:
@@ -36,6 +36,8 @@ def _evaluate(value, params: Dict):
     expr = sp.sympify(value)
     subs = {}
     for s in expr.free_symbols:
+        if s.name not in params and placeholder is not None:
+            return float(placeholder)
         if s.name not in params:
             raise ValueError(f"kernel parameter {s.name!r} has no value: pass {s.name}=... when calling the kernel")
         subs[s] = params[s.name]
@@ -54,8 +56,10 @@ def free_parameters(update_rule) -> set:
     return names
 
 
-def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None) -> N.LbmPlanDesc:
-    """Resolves an update rule plus parameter values into the C plan descriptor."""
+def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None,
+               rates_needed: bool = True) -> N.LbmPlanDesc:
+    """Resolves an update rule plus parameter values into the C plan descriptor.  Plans that only
+    run the getter / setter do not need relaxation rates (rates_needed=False)."""
     rule = update_rule.collision_rule
     m = rule.method
     d = N.LbmPlanDesc()
@@ -65,7 +69,8 @@ def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None) -
     d.pattern = _PATTERN[update_rule.streaming_pattern]
     d.compressible = int(bool(m.compressible))
     d.continuous_equilibrium = int(bool(m.continuous_equilibrium))
-    rates = [_evaluate(r, params) for r in m.relaxation_rates]
+    ph = None if rates_needed else 1.0
+    rates = [_evaluate(r, params, ph) for r in m.relaxation_rates]
     if m.kind in ("srt", "trt"):
         from . import methods as M
         monos = M.default_monomials(m.stencil.name)
@@ -83,7 +88,7 @@ def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None) -
         for k in range(3):
             d.force[k] = f[k]
     d.galilean_correction = int(bool(rule.galilean_correction))
-    shear = _evaluate(m.shear_relaxation_rate, params)
+    shear = _evaluate(m.shear_relaxation_rate, params, ph)
     d.shear_rate = shear
     if rule.subgrid_scale_model is not None:
         d.sgs = N.SGS_SMAGORINSKY
@@ -113,6 +118,33 @@ def _stream_handle(stream) -> Optional[int]:
     return int(stream)
 
 
+class BoundSweep:
+    """A sweep with its plan, strides, flags and stream resolved once: launching it costs one
+    ctypes call (the per-step path of LatticeBoltzmannStep)."""
+
+    def __init__(self, plan: N.Plan, strides, flags, stream_handle):
+        self.plan = plan
+        self._strides = N.i64_array(strides)
+        self._flags = ctypes.c_void_p(flags.data_ptr() if flags is not None else None)
+        self._flags_ref = flags
+        self._stream = ctypes.c_void_p(stream_handle)
+        self._lib = N.lib()
+
+    def sweep(self, src_ptr: int, dst_ptr: int, parity: int):
+        rc = self._lib.lbm_sweep(self.plan.handle, ctypes.c_void_p(src_ptr), ctypes.c_void_p(dst_ptr),
+                                 self._strides, self._flags, parity, None, self._stream)
+        if rc:
+            N.check(rc, "lbm_sweep")
+
+    def run(self, a_ptr: int, b_ptr: int, first_parity: int, steps: int) -> bool:
+        """`steps` sweeps in one call; returns True if a pull result ended in `b`."""
+        in_b = ctypes.c_int(0)
+        N.check(self._lib.lbm_run(self.plan.handle, ctypes.c_void_p(a_ptr), ctypes.c_void_p(b_ptr),
+                                  self._strides, self._flags, first_parity, int(steps), ctypes.byref(in_b),
+                                  self._stream), "lbm_run")
+        return bool(in_b.value)
+
+
 class LbKernel:
     def __init__(self, update_rule):
         self.update_rule = update_rule
@@ -134,6 +166,13 @@ class LbKernel:
         elif bytes(p.desc) != bytes(desc):
             p.update(desc)
         return p
+
+    def bind(self, pdfs: torch.Tensor, periodic, flags=None, ubb_velocities=None, params=None,
+             stream=None) -> BoundSweep:
+        check_pdf_tensor(pdfs, self.q, self.update_rule.storage_dtype, "pdfs")
+        dims = [s - 2 for s in pdfs.shape[:3]]
+        plan = self.plan(dims, periodic, params or {}, ubb_velocities)
+        return BoundSweep(plan, pdfs.stride(), flags, _stream_handle(stream))
 
     def _parity(self):
         ts = self.update_rule.timestep

@@ -103,6 +103,7 @@ class LatticeBoltzmannStep:
         self._macro = _MacroPlanCache(self.method, self.streaming_pattern, self._kernels[0].update_rule.collision_rule)
         # parity of the last completed step: in-place patterns start as if an ODD step just ran
         self._prev = Timestep.ODD if self._inplace else Timestep.BOTH
+        self._bound_sweep = None
         self.time_steps_run = 0
         self.set_pdf_fields_from_macroscopic_values()
 
@@ -185,6 +186,20 @@ class LatticeBoltzmannStep:
                            self._boundary_handling.ubb_velocities)
         return self._boundary_handling.flags(plan)
 
+    def _bound(self):
+        """The sweep with plan, strides, flags and stream resolved; rebuilt when boundaries,
+        kernel parameters or the current stream change."""
+        bh = self._boundary_handling
+        key = (id(bh._dev), bh._dev is None, tuple(sorted(self.kernel_params.items())),
+               torch.cuda.current_stream().cuda_stream)
+        if getattr(self, "_bound_key", None) != key or self._bound_sweep is None:
+            k = self._kernels[0]
+            flags = self._flags(k)
+            self._bound_sweep = k.bind(self.pdfs, self.periodicity, flags, bh.ubb_velocities, self.kernel_params)
+            self._bound_key = (id(bh._dev), bh._dev is None, tuple(sorted(self.kernel_params.items())),
+                               torch.cuda.current_stream().cuda_stream)
+        return self._bound_sweep
+
     def set_pdf_fields_from_macroscopic_values(self):
         rho = torch.from_numpy(np.ascontiguousarray(self._density)).to(self.device)
         u = torch.from_numpy(np.ascontiguousarray(self._velocity)).to(self.device)
@@ -194,20 +209,32 @@ class LatticeBoltzmannStep:
         pass
 
     def time_step(self):
+        b = self._bound()
         if self._inplace:
             nxt = self._prev.next()
-            k = self._kernels[nxt.idx]
-            k(src=self.pdfs, flags=self._flags(k), ubb_velocities=self._boundary_handling.ubb_velocities,
-              periodicity=self.periodicity, **self.kernel_params)
+            p = self.pdfs.data_ptr()
+            b.sweep(p, p, int(nxt.idx))
             self._prev = nxt
         else:
-            k = self._kernels[0]
-            fn = k.update_rule
-            k(**{fn.field_name: self.pdfs, fn.temporary_field_name: self.pdfs_tmp}, flags=self._flags(k),
-              ubb_velocities=self._boundary_handling.ubb_velocities, periodicity=self.periodicity,
-              **self.kernel_params)
+            b.sweep(self.pdfs.data_ptr(), self.pdfs_tmp.data_ptr(), 0)
             self.pdfs, self.pdfs_tmp = self.pdfs_tmp, self.pdfs
         self.time_steps_run += 1
+
+    def run_sweeps(self, time_steps):
+        """`time_steps` sweeps launched from one C call (no per-step Python), no getter."""
+        n = int(time_steps)
+        if n <= 0:
+            return
+        b = self._bound()
+        if self._inplace:
+            nxt = self._prev.next()
+            p = self.pdfs.data_ptr()
+            b.run(p, p, int(nxt.idx), n)
+            self._prev = Timestep((int(nxt.idx) + n - 1) % 2)
+        else:
+            if b.run(self.pdfs.data_ptr(), self.pdfs_tmp.data_ptr(), 0, n):
+                self.pdfs, self.pdfs_tmp = self.pdfs_tmp, self.pdfs
+        self.time_steps_run += n
 
     def post_run(self):
         cd = torch.float64 if self._compute == "float64" else torch.float32
@@ -219,8 +246,7 @@ class LatticeBoltzmannStep:
 
     def run(self, time_steps):
         self.pre_run()
-        for _ in range(int(time_steps)):
-            self.time_step()
+        self.run_sweeps(time_steps)
         self.post_run()
 
     def benchmark_run(self, time_steps, number_of_cells=None):
@@ -230,8 +256,7 @@ class LatticeBoltzmannStep:
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         start.record()
-        for _ in range(int(time_steps)):
-            self.time_step()
+        self.run_sweeps(time_steps)
         stop.record()
         torch.cuda.synchronize()
         seconds = start.elapsed_time(stop) * 1e-3 / max(int(time_steps), 1)

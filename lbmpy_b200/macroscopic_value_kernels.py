@@ -43,7 +43,7 @@ class _MacroPlanCache:
         dims = tuple(int(s) - 2 for s in pdfs.shape[:3])
         key = (storage, dims, tuple(periodicity), torch.cuda.current_device())
         rule = _rule_for(self.lb_method, self.pattern, storage, self.collision_rule)
-        desc = build_desc(rule, dims, periodicity, params or {})
+        desc = build_desc(rule, dims, periodicity, params or {}, rates_needed=False)
         p = self._plans.get(key)
         if p is None:
             p = N.Plan(desc)
@@ -76,7 +76,7 @@ def set_equilibrium(plan_cache, pdfs, density, velocity, previous_timestep=Times
     m = plan_cache.lb_method
     check_pdf_tensor(pdfs, m.stencil.Q, dtype_name(pdfs.dtype))
     dims = tuple(int(s) - 2 for s in pdfs.shape[:3])
-    cd = _compute_dtype(pdfs)
+    cd = torch.float64          # the setter evaluates the equilibrium in FP64 for every storage type
     dev = pdfs.device
     if isinstance(density, torch.Tensor):
         rho = _interior(density.to(device=dev, dtype=cd), dims)
