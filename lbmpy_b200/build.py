@@ -43,10 +43,11 @@ def flags(verbose=False) -> list:
     return f
 
 
-def _digest() -> str:
+def _digest(source: str = None) -> str:
+    """Hash of the shared headers, the compiler flags and one source (or all sources)."""
     h = hashlib.sha256()
     for name in sorted(os.listdir(CSRC)):
-        if name.endswith((".cu", ".cuh", ".h")):
+        if name.endswith((".cuh", ".h")) or (name.endswith(".cu") and (source is None or name == source)):
             with open(os.path.join(CSRC, name), "rb") as fh:
                 h.update(name.encode() + fh.read())
     with open(os.path.join(HERE, "..", "include", "lbm_b200.h"), "rb") as fh:
@@ -67,10 +68,16 @@ def build(verbose: bool = False, force: bool = False) -> str:
 
     def compile_one(src):
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+        ostamp = obj + ".stamp"
+        d = _digest(src)
+        if not force and not verbose and os.path.exists(obj) and os.path.exists(ostamp) and open(ostamp).read() == d:
+            return obj, ""
         cmd = [cc, "-c", os.path.join(CSRC, src), "-o", obj] + flags(verbose)
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
+        with open(ostamp, "w") as fh:
+            fh.write(d)
         return obj, r.stderr
 
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
