@@ -116,6 +116,16 @@ int lbm_get_macroscopic(const LbmPlan* plan, const void* pdfs, const int64_t str
 int lbm_reduce_conserved(const LbmPlan* plan, const void* pdfs, const int64_t strides[4],
                          const uint8_t* flags, int prev_parity, double out[5], void* stream);
 
+/* Same sums as lbm_reduce_conserved, for callers that cannot allocate device memory: it takes
+ * the plan description instead of a plan and keeps its partial sums in a static device array of
+ * 2048 x 5 doubles (80 KiB per GPU, resident until exit), calling no cudaMalloc / cudaFree.
+ * No counterpart in the reference.  Fails with LBM_E_INVALID if the launch would need more than
+ * 2048 partial sums (more than 512 SMs).  Calls that overlap on the GPU share the array and race.
+ * The first call on a device resolves the array's address; make it before any stream capture.
+ * Waits for its result. */
+int lbm_reduce_conserved_noalloc(const LbmPlanDesc* desc, const void* pdfs, const int64_t strides[4],
+                                 const uint8_t* flags, int prev_parity, double out[5], void* stream);
+
 /* Sets bit 7 on every fluid cell of `flags` (device, layout above) that has a boundary
  * neighbour along the plan's stencil, honouring periodicity.  Replaces the link-list setup of
  * LatticeBoltzmannBoundaryHandling (boundaries/boundaryhandling.py:15-155). */

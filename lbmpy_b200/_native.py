@@ -20,8 +20,8 @@ SGS_NONE, SGS_SMAGORINSKY = 0, 1
 
 # exported symbols, one per declaration in include/lbm_b200.h
 EXPORTS = ("lbm_plan_create", "lbm_plan_destroy", "lbm_plan_update", "lbm_sweep", "lbm_run",
-           "lbm_set_equilibrium", "lbm_get_macroscopic", "lbm_reduce_conserved", "lbm_flags_finalize",
-           "lbm_last_error", "lbm_version")
+           "lbm_set_equilibrium", "lbm_get_macroscopic", "lbm_reduce_conserved", "lbm_reduce_conserved_noalloc",
+           "lbm_flags_finalize", "lbm_last_error", "lbm_version")
 
 
 class LbmPlanDesc(ctypes.Structure):
@@ -67,6 +67,8 @@ def lib():
         L.lbm_set_equilibrium.argtypes = [vp, vp, i64p, vp, i64p, vp, i64p, ctypes.c_int, vp]
         L.lbm_get_macroscopic.argtypes = [vp, vp, i64p, vp, i64p, vp, i64p, ctypes.c_int, vp]
         L.lbm_reduce_conserved.argtypes = [vp, vp, i64p, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), vp]
+        L.lbm_reduce_conserved_noalloc.argtypes = [ctypes.POINTER(LbmPlanDesc), vp, i64p, vp, ctypes.c_int,
+                                                   ctypes.POINTER(ctypes.c_double), vp]
         L.lbm_flags_finalize.argtypes = [vp, vp, vp]
         L.lbm_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTS:

@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "../../include/lbm_b200.h"
@@ -497,3 +498,89 @@ int lbm_flags_finalize(const LbmPlan* p, uint8_t* flags, void* stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free variant of lbm_reduce_conserved.
+//
+// Some callers cannot call cudaMalloc at all: code running where device allocation is forbidden
+// or must stay predictable (inside a fixed memory budget, an allocator-less embedding, or a
+// process whose memory is all pre-reserved by another framework).  For them this entry point
+// takes the plan description instead of a plan (lbm_plan_create allocates the reduction
+// scratch) and keeps its block partial sums in a file-scope device array instead.
+//
+// Capacity: LBM_NOALLOC_MAX_BLOCKS partial sums of 5 doubles (80 KiB).  The launch uses at most
+// 4 blocks per SM; a call that would need more partials than the array holds is rejected.  The
+// array exists once per GPU that loads the library, for the life of the process.  Every call
+// overwrites the partials it reads, so no state carries over between calls, but calls that
+// overlap on the GPU (different streams, or concurrent host threads) share the array and race.
+// The first call on a device resolves the array's device address (cudaGetSymbolAddress); make
+// that first call before any stream capture on that device.
+static constexpr int LBM_NOALLOC_MAX_BLOCKS = 2048;
+static __device__ __align__(256) double g_noalloc_scratch[LBM_NOALLOC_MAX_BLOCKS * 5 + 5];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kMaxDevices] = {};
+
+int noalloc_scratch(int device, double** out) {
+    if (device < 0 || device >= kMaxDevices) return fail(LBM_E_DEVICE, "device index %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_ptr[device] == nullptr) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);   // the current device's copy
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(reduction scratch)");
+        g_noalloc_ptr[device] = static_cast<double*>(ptr);
+    }
+    *out = g_noalloc_ptr[device];
+    return LBM_OK;
+}
+}  // namespace
+
+extern "C" int lbm_reduce_conserved_noalloc(const LbmPlanDesc* desc, const void* pdfs, const int64_t strides[4],
+                                            const uint8_t* flags, int prev_parity, double out[5], void* stream) {
+    if (desc == nullptr || out == nullptr) return fail(LBM_E_INVALID, "desc and out must not be NULL");
+    int rc = validate_desc(desc);
+    if (rc) return rc;
+    LbmPlan p;                                   // on the stack: nothing is allocated
+    memset(&p, 0, sizeof(p));
+    p.desc = *desc;
+    cudaError_t e = cudaGetDevice(&p.device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    p.q = desc->stencil;
+    p.mk = desc->method == LBM_METHOD_MRT ? MK_MRT : (desc->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
+    p.store = desc->store_dtype;
+    fill_physics(&p, desc);
+    MacroArgs a;
+    if ((rc = macro_common(&p, pdfs, strides, nullptr, nullptr, nullptr, nullptr, a))) return rc;
+    if ((rc = check_device_ptr(&p, flags, "flags", true))) return rc;
+    a.g.flags = flags;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+    const long long cells = (long long)desc->dims[0] * desc->dims[1] * desc->dims[2];
+    const long long wanted = (cells + RED_THREADS - 1) / RED_THREADS;
+    const int blocks = (int)(wanted < (long long)sms * 4 ? wanted : (long long)sms * 4);
+    if (blocks > LBM_NOALLOC_MAX_BLOCKS)
+        return fail(LBM_E_INVALID,
+                    "lbm_reduce_conserved_noalloc needs %d partial sums but its static scratch holds %d "
+                    "(at most 4 blocks per SM on up to %d SMs)", blocks, LBM_NOALLOC_MAX_BLOCKS,
+                    LBM_NOALLOC_MAX_BLOCKS / 4);
+    double* scratch = nullptr;
+    if ((rc = noalloc_scratch(p.device, &scratch))) return rc;
+    double* partial = scratch;
+    double* result = scratch + 5 * LBM_NOALLOC_MAX_BLOCKS;
+    const int pat = pattern_kind(&p, prev_parity ? 1 : 0);
+    ReduceLauncher L = p.q == 19 ? reduce_launcher_q<19>(p.store, pat) : reduce_launcher_q<27>(p.store, pat);
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no reduction kernel for this storage type / pattern");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    e = L(a, blocks, partial, s);
+    if (e != cudaSuccess) return cuda_fail(e, "reduction launch");
+    k_reduce_finish<<<1, 32, 0, s>>>(partial, blocks, result);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "reduction finish launch");
+    e = cudaMemcpyAsync(out, result, 5 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(e, "reduction copy");
+    e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "reduction sync");
+}
