@@ -98,6 +98,54 @@ class ClockSampler:
                 "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
+def make_d3q19_tgv(device, n, storage, seed=0, method="trt", pattern="pull"):
+    """D3Q19 periodic box, Taylor-Green vortex u0 = 0.04 plus Gaussian noise 1e-3 (seeded)."""
+    import lbmpy_b200 as L
+    compute = "float64" if storage == "float64" else "float32"
+    kw = dict(relaxation_rate=1.8) if method == "trt" else dict(relaxation_rates=[1.8, 1.6, 1.0, 1.0])
+    step = L.LatticeBoltzmannStep(domain_size=(n, n, n), periodicity=True, stencil=L.Stencil.D3Q19,
+                                  method=getattr(L.Method, method.upper()), compressible=True,
+                                  streaming_pattern=pattern, config=L.CreateKernelConfig(data_type=compute),
+                                  optimization={"storage_dtype": storage}, device=device, **kw)
+    x = np.arange(n)
+    k = 2 * np.pi / n
+    u = np.zeros((n, n, n, 3))
+    u[..., 0] = (0.04 * np.sin(k * x)[:, None] * np.cos(k * x)[None, :])[:, :, None]
+    u[..., 1] = (-0.04 * np.cos(k * x)[:, None] * np.sin(k * x)[None, :])[:, :, None]
+    u += 1e-3 * np.random.default_rng(seed).standard_normal(u.shape, dtype=np.float32)
+    step.velocity_array[...] = u
+    step.set_pdf_fields_from_macroscopic_values()
+    return step
+
+
+# name -> (factory(device), cells per sweep, populations per cell, bytes per stored population)
+WORKLOADS = {
+    "d3q27-cumulant-aa-channel-256x128x128": (lambda dev: make_channel(dev), SHAPE[0] * SHAPE[1] * SHAPE[2], 27, 4),
+}
+for _n in (64, 256, 512):
+    for _st, _isz in (("float64", 8), ("float32", 4), ("float16", 2), ("bfloat16", 2)):
+        WORKLOADS[f"d3q19-trt-pull-{_st}-{_n}"] = (
+            (lambda dev, n=_n, st=_st: make_d3q19_tgv(dev, n, st)), _n ** 3, 19, _isz)
+    WORKLOADS[f"d3q19-mrt-pull-float32-{_n}"] = (
+        (lambda dev, n=_n: make_d3q19_tgv(dev, n, "float32", method="mrt")), _n ** 3, 19, 4)
+    WORKLOADS[f"d3q19-trt-aa-float32-{_n}"] = (
+        (lambda dev, n=_n: make_d3q19_tgv(dev, n, "float32", pattern="aa")), _n ** 3, 19, 4)
+
+
+def make_cavity_batch(device, n_cavities=512, seed=0):
+    """512 independent lid-driven cavities (D3Q19 MRT, FP32, pull), edges seeded from
+    {16, 24, ..., 96} per axis, shear/bulk rates seeded uniform in [1.5, 1.95], lid 0.05; one
+    persistent launch per step over all cavities, tiling autotuned, steps replayed from a CUDA
+    graph."""
+    from lbmpy_b200.batched import lid_driven_cavity_batch
+    b = lid_driven_cavity_batch(n_cavities, seed=seed, device=device)
+    b.finalize()
+    return b
+
+
+WORKLOADS["batched-ldc-512-d3q19-mrt-float32"] = (lambda dev: make_cavity_batch(dev), None, 19, 4)
+
+
 def make_channel(device, shape=SHAPE, seed=0):
     """The channel through the lbmpy-compatible API (create_channel-style set-up, AA in place)."""
     import lbmpy_b200 as L
@@ -184,6 +232,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--workload", default="d3q27-cumulant-aa-channel-256x128x128", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -202,11 +252,16 @@ def main():
 
     from lbmpy_b200 import _native
     _native.lib()
-    step = make_channel(device)
-    cells = SHAPE[0] * SHAPE[1] * SHAPE[2]
+    factory, cells, q_pop, itemsize = WORKLOADS[args.workload]
+    step = factory(device)
+    cells = step.number_of_cells
+    headline = args.workload == "d3q27-cumulant-aa-channel-256x128x128"
+    batched = args.workload.startswith("batched")
     warm = max(args.warmup, 3)
     for _ in range(warm + (warm % 2)):
         step.time_step()
+    if batched:
+        step.run_sweeps(args.steps)          # captures the graph of K launches that is timed below
     torch.cuda.synchronize()
 
     stream = torch.cuda.current_stream()
@@ -216,8 +271,11 @@ def main():
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         start.record(stream)
-        for _ in range(args.steps):
-            step.time_step()
+        if batched:
+            step.run_sweeps(args.steps)      # one graph replay: K persistent launches
+        else:
+            for _ in range(args.steps):
+                step.time_step()
         stop.record(stream)
         torch.cuda.synchronize()
     if world > 1:
@@ -232,7 +290,7 @@ def main():
 
     # roofline of the sweep kernel (the only kernel in the timed region)
     peak, peak_kind = measured_peak()
-    achieved = algorithmic_bytes_per_sweep(cells) / (ms / args.steps * 1e-3) / 1e9
+    achieved = algorithmic_bytes_per_sweep(cells, q_pop, itemsize) / (ms / args.steps * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     if os.path.exists(tpath):
@@ -241,7 +299,7 @@ def main():
 
     # end to end through the public API: host PDFs in, run, PDFs and macroscopic fields out
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and headline:
         pdf_bytes = step.pdfs.untyped_storage().nbytes()
         pinned = torch.empty(pdf_bytes // 4, dtype=torch.float32, pin_memory=True)
         dev_flat = torch.empty(pdf_bytes // 4, dtype=torch.float32, device=device)
@@ -280,23 +338,55 @@ def main():
                "call": "PDFs host->device, 100 x LatticeBoltzmannStep.time_step(), getter, PDFs+rho+u device->host"}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and headline:
         cpu = cpu_baseline_sample()
 
+    secondary = None
+    if headline and rank == 0 and world == 1 and not args.no_secondary:
+        # FP16 / BF16 storage against FP32 on the 512^3 D3Q19 TRT periodic box (same kernel family)
+        del step
+        torch.cuda.empty_cache()
+        secondary = {}
+        for name in ("d3q19-trt-pull-float32-512", "d3q19-trt-pull-float16-512", "d3q19-trt-pull-bfloat16-512"):
+            f2, c2, q2, i2 = WORKLOADS[name]
+            st2 = f2(device)
+            for _ in range(4):
+                st2.time_step()
+            a2, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a2.record(stream)
+            st2.run_sweeps(20)
+            b2.record(stream)
+            torch.cuda.synchronize()
+            ms2 = a2.elapsed_time(b2) / 20
+            g2 = c2 / (ms2 * 1e-3) / 1e9
+            secondary[name] = {"GLUPS": g2, "GB/s": g2 * 2 * q2 * i2, "frac": g2 * 2 * q2 * i2 / peak}
+            del st2
+            torch.cuda.empty_cache()
+        secondary["fp16_over_fp32"] = (secondary["d3q19-trt-pull-float16-512"]["GLUPS"] /
+                                       secondary["d3q19-trt-pull-float32-512"]["GLUPS"])
+
     if rank == 0:
-        line = {"metric": "D3Q27 cumulant channel GLUPS", "value": glups, "unit": "GLUPS", "n_gpus": world,
+        line = {"metric": "D3Q19/D3Q27 GLUPS and % of HBM roofline; FP16-store vs FP32 at equal L2 error",
+                "value": glups, "unit": "GLUPS", "n_gpus": world,
                 "steps": args.steps, "warmup": warm + (warm % 2), "ms_per_step": ms_per_step,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic",
-                "config": {"workload": "d3q27-cumulant-aa-channel-256x128x128", "shape": list(SHAPE),
-                           "omega": OMEGA, "force": FORCE, "pattern": "aa", "galilean_correction": True,
-                           "storage": "float32 zero-centred", "parallelism": f"replicas{world}",
-                           "l2": "inputs larger than L2 (453 MB PDF field vs 126 MB L2)"},
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": {8: "f64", 4: "f32", 2: "f32 (16-bit storage)"}[itemsize], "data": "synthetic",
+                "config": {"workload": args.workload, "cells": cells, "populations": q_pop,
+                           "bytes_per_population": itemsize, "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2" if cells * q_pop * itemsize > 126e6
+                           else "inputs fit in L2 (no flush)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                             "bytes_per_lu": 2 * Q * 4},
+                             "bytes_per_lu": 2 * q_pop * itemsize},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
-                "clocks": clocks.summary()}
+                "clocks": clocks.summary(), "secondary": secondary}
+        if batched:
+            line["config"].update({"domains": step.n_domains, "tiling": vars(step.tiling), **step.info(),
+                                   "graph": "K launches captured in one CUDA graph, replayed once"})
+        if headline:
+            line["config"].update({"shape": list(SHAPE), "omega": OMEGA, "force": FORCE, "pattern": "aa",
+                                   "galilean_correction": True, "storage": "float32 zero-centred"})
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -131,6 +131,49 @@ int lbm_reduce_conserved_noalloc(const LbmPlanDesc* desc, const void* pdfs, cons
  * LatticeBoltzmannBoundaryHandling (boundaries/boundaryhandling.py:15-155). */
 int lbm_flags_finalize(const LbmPlan* plan, uint8_t* flags, void* stream);
 
+/* ---- Batched domains: many independent fields of uneven size in one persistent launch ----
+ * No single lbmpy counterpart: lbmpy runs one LatticeBoltzmannStep (lbstep.py:18-450) per
+ * domain; a batch replaces a loop over such steps.  Every domain owns a ghost-layered field at
+ * `offset` elements into each of the two shared buffers (pull ping-pongs between them; in-place
+ * patterns use buffer a only), its flags at `flags_offset` bytes into the shared flag buffer
+ * (-1: none; same layout as for lbm_sweep), and its own relaxation rates and UBB velocities.
+ * Everything else (stencil, method, dtype, pattern, force, SGS) comes from `common`, whose
+ * dims, periodic, rates and ubb_velocity are ignored. */
+typedef struct LbmDomainDesc {
+    int32_t dims[3];
+    int32_t periodic[3];
+    int64_t strides[4];         /* {1, sy, sz, sq} elements */
+    int64_t offset;             /* element offset of the field in buffer a and in buffer b */
+    int64_t flags_offset;       /* byte offset into the flag buffer, or -1 */
+    double rates[27];
+    double ubb_velocity[4][3];
+} LbmDomainDesc;
+
+typedef struct LbmBatch LbmBatch;
+
+/* How the persistent launch walks the domains: blocks of tile_x x tile_y threads
+ * (tile_x * tile_y <= 256), each thread updating up to cells_z cells along z, and
+ * blocks_per_sm x (number of SMs) blocks striding over the tiles (0: one block per tile). */
+typedef struct LbmBatchTiling {
+    int32_t tile_x, tile_y, cells_z, blocks_per_sm;
+} LbmBatchTiling;
+
+/* Validates every domain (bounds inside buffers of buffer_elems elements and a flag buffer of
+ * flags_bytes bytes, no two domains overlapping), marks the near-wall cells of every domain's
+ * flags in place (as lbm_flags_finalize), uploads the per-domain arguments and the tile table.
+ * In-place patterns take buffer_b == NULL or buffer_a.  The buffers stay owned by the caller. */
+int lbm_batch_create(const LbmPlanDesc* common, const LbmDomainDesc* domains, int n_domains, void* buffer_a,
+                     void* buffer_b, int64_t buffer_elems, uint8_t* flags, int64_t flags_bytes,
+                     const LbmBatchTiling* tiling, LbmBatch** out);
+/* One sweep of every domain.  Pull: parity 0 reads a and writes b, parity 1 the reverse.
+ * AA: the parity of this step.  Makes no host-side check or synchronisation, so it can be
+ * captured in a CUDA graph. */
+int lbm_batch_sweep(const LbmBatch* batch, int parity, void* stream);
+/* info = {tiles, blocks launched, interior cells over all domains, thread slots (tiles x tile
+ * cells)}. */
+int lbm_batch_info(const LbmBatch* batch, int64_t info[4]);
+int lbm_batch_destroy(LbmBatch* batch);
+
 /* Copies the message of the last failed call on this thread into buf (NUL-terminated). */
 int lbm_last_error(char* buf, size_t n);
 

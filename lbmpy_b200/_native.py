@@ -21,7 +21,8 @@ SGS_NONE, SGS_SMAGORINSKY = 0, 1
 # exported symbols, one per declaration in include/lbm_b200.h
 EXPORTS = ("lbm_plan_create", "lbm_plan_destroy", "lbm_plan_update", "lbm_sweep", "lbm_run",
            "lbm_set_equilibrium", "lbm_get_macroscopic", "lbm_reduce_conserved", "lbm_reduce_conserved_noalloc",
-           "lbm_flags_finalize", "lbm_last_error", "lbm_version")
+           "lbm_flags_finalize", "lbm_batch_create", "lbm_batch_sweep", "lbm_batch_info", "lbm_batch_destroy",
+           "lbm_last_error", "lbm_version")
 
 
 class LbmPlanDesc(ctypes.Structure):
@@ -41,6 +42,19 @@ class LbmPlanDesc(ctypes.Structure):
         ("dims", ctypes.c_int32 * 3),
         ("periodic", ctypes.c_int32 * 3),
     ]
+
+
+class LbmDomainDesc(ctypes.Structure):
+    _fields_ = [
+        ("dims", ctypes.c_int32 * 3), ("periodic", ctypes.c_int32 * 3),
+        ("strides", ctypes.c_int64 * 4), ("offset", ctypes.c_int64), ("flags_offset", ctypes.c_int64),
+        ("rates", ctypes.c_double * 27), ("ubb_velocity", (ctypes.c_double * 3) * 4),
+    ]
+
+
+class LbmBatchTiling(ctypes.Structure):
+    _fields_ = [("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32), ("cells_z", ctypes.c_int32),
+                ("blocks_per_sm", ctypes.c_int32)]
 
 
 class LbmError(RuntimeError):
@@ -70,6 +84,12 @@ def lib():
         L.lbm_reduce_conserved_noalloc.argtypes = [ctypes.POINTER(LbmPlanDesc), vp, i64p, vp, ctypes.c_int,
                                                    ctypes.POINTER(ctypes.c_double), vp]
         L.lbm_flags_finalize.argtypes = [vp, vp, vp]
+        L.lbm_batch_create.argtypes = [ctypes.POINTER(LbmPlanDesc), ctypes.POINTER(LbmDomainDesc), ctypes.c_int, vp,
+                                       vp, ctypes.c_int64, vp, ctypes.c_int64, ctypes.POINTER(LbmBatchTiling),
+                                       ctypes.POINTER(ctypes.c_void_p)]
+        L.lbm_batch_sweep.argtypes = [vp, ctypes.c_int, vp]
+        L.lbm_batch_info.argtypes = [vp, i64p]
+        L.lbm_batch_destroy.argtypes = [vp]
         L.lbm_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTS:
             getattr(L, name).restype = ctypes.c_int

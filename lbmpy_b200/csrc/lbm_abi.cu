@@ -3,10 +3,14 @@
 #include <cuda_runtime.h>
 
 #include <cstdarg>
+#include <cstdint>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/lbm_b200.h"
 #include "lbm_dispatch.h"
@@ -17,6 +21,7 @@ struct LbmPlan {
     LbmPlanDesc desc;
     int device;
     int q, mk, store;
+    int use_pair;          // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_PAIR)
     Physics phys;
     double* partial;       // reduction scratch: RED_BLOCKS * 5 doubles
     double* red_out;       // 5 doubles on the device
@@ -125,6 +130,41 @@ SweepLauncher sweep_launcher(const LbmPlan* p, int pat) {
     if (p->q == 27 && p->mk == MK_CUM) return sweep_q27_cum(p->store, pat);
     if (p->q == 27 && p->mk == MK_CUM1) return sweep_q27_cum1(p->store, pat);
     return nullptr;
+}
+
+SweepLauncher pair_launcher(const LbmPlan* p, int pat) {
+    if (p->q == 19 && p->mk == MK_POP) return sweep_pair_q19_pop(p->store, pat);
+    if (p->q == 19 && p->mk == MK_MRT) return sweep_pair_q19_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_POP) return sweep_pair_q27_pop(p->store, pat);
+    if (p->q == 27 && p->mk == MK_MRT) return sweep_pair_q27_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM) return sweep_pair_q27_cum(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM1) return sweep_pair_q27_cum1(p->store, pat);
+    return nullptr;
+}
+
+size_t store_size(int store) { return store == ST_F64 ? 8 : (store == ST_F32 ? 4 : 2); }
+
+// The pair sweep needs an even row length, no omega output, and every row's interior cell x = 0
+// (ghost-inclusive x = 1) on a 2-element boundary so that paired loads / stores are aligned.
+// Default policy, from B200 measurements: the pair sweep wins where the one-cell sweep is limited by
+// instruction issue (16-bit storage, the cumulant with pull streaming); for FP32 storage the
+// one-cell sweep already streams at HBM speed and keeps twice the occupancy.
+bool pair_preferred(const LbmPlan* p, int pat) {
+    if (p->use_pair >= 0) return p->use_pair == 1;
+    if (p->store == ST_F16 || p->store == ST_BF16) return true;
+    return (p->mk == MK_CUM || p->mk == MK_CUM1) && pat == PAT_PULL;
+}
+
+bool pair_applicable(const LbmPlan* p, const void* src, const void* dst, const int64_t s[4], int pat,
+                     const float* omega_out) {
+    if (!pair_preferred(p, pat) || p->store == ST_F64 || omega_out != nullptr) return false;
+    if (pat != PAT_PULL && pat != PAT_AA_EVEN && pat != PAT_AA_ODD) return false;
+    if (p->desc.dims[0] % 2 != 0) return false;
+    const size_t es = store_size(p->store);
+    if ((reinterpret_cast<uintptr_t>(src) + es) % (2 * es) != 0) return false;
+    if ((reinterpret_cast<uintptr_t>(dst) + es) % (2 * es) != 0) return false;
+    if (s[1] % 2 != 0 || s[2] % 2 != 0 || s[3] % 2 != 0) return false;
+    return pair_launcher(p, pat) != nullptr;
 }
 
 MacroLauncher set_eq_launcher(const LbmPlan* p, int pat) {
@@ -304,6 +344,10 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
     p->mk = desc->method == LBM_METHOD_MRT ? MK_MRT : (desc->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
     if (p->mk == MK_CUM && cumulant_high_orders_relax_to_equilibrium(desc)) p->mk = MK_CUM1;
     p->store = desc->store_dtype;
+    {
+        const char* env = getenv("LBM_B200_PAIR");
+        p->use_pair = env == nullptr ? -1 : (env[0] == '0' ? 0 : 1);
+    }
     fill_physics(p, desc);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
@@ -362,8 +406,6 @@ static int validate_sweep(const LbmPlan* p, const void* src, const void* dst, co
 static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, const int64_t strides[4],
                                 const uint8_t* flags, int parity, float* omega_out, cudaStream_t stream) {
     const int pat = pattern_kind(p, parity);
-    SweepLauncher L = sweep_launcher(p, pat);
-    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no kernel for this storage type / pattern");
     SweepArgs a;
     a.g = make_grid(p, strides, flags);
     a.p = p->phys;
@@ -371,7 +413,16 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
     a.dst = dst;
     a.omega_out = omega_out;
     dim3 grid, block;
-    launch_shape(a.g, grid, block);
+    SweepLauncher L;
+    if (pair_applicable(p, src, dst, strides, pat, omega_out)) {
+        L = pair_launcher(p, pat);
+        block = dim3(32, PAIR_ROWS, 1);
+        grid = dim3((a.g.nx + 63) / 64, (a.g.ny + PAIR_ROWS - 1) / PAIR_ROWS, a.g.nz);
+    } else {
+        L = sweep_launcher(p, pat);
+        launch_shape(a.g, grid, block);
+    }
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no kernel for this storage type / pattern");
     cudaError_t e = L(a, grid, block, stream);
     if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
     return LBM_OK;
@@ -495,6 +546,238 @@ int lbm_flags_finalize(const LbmPlan* p, uint8_t* flags, void* stream) {
     else k_flags_finalize<27><<<grid, block, 0, st>>>(g);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? LBM_OK : cuda_fail(e, "flag finalize launch");
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Batched domains: one persistent launch per step over a tile table spanning every domain.
+
+struct LbmBatch {
+    int device;
+    int q, mk, store, pattern;
+    int n_domains;
+    LbmBatchTiling tiling;
+    int64_t n_tiles, grid_blocks, cells;
+    SweepArgs* d_domains;      // [2][n_domains]: parity 0 and parity 1 source/destination
+    BatchTile* d_tiles;
+};
+
+namespace {
+
+BatchLauncher batched_launcher(int q, int mk, int store, int pat) {
+    if (q == 19 && mk == MK_POP) return batched_q19_pop(store, pat);
+    if (q == 19 && mk == MK_MRT) return batched_q19_mrt(store, pat);
+    if (q == 27 && mk == MK_POP) return batched_q27_pop(store, pat);
+    if (q == 27 && mk == MK_MRT) return batched_q27_mrt(store, pat);
+    if (q == 27 && mk == MK_CUM) return batched_q27_cum(store, pat);
+    if (q == 27 && mk == MK_CUM1) return batched_q27_cum1(store, pat);
+    return nullptr;
+}
+
+// The plan-shaped view of one domain, for the shared validation and physics helpers.
+void domain_plan(const LbmPlanDesc* common, const LbmDomainDesc& d, int device, LbmPlan& p) {
+    p.desc = *common;
+    memcpy(p.desc.dims, d.dims, sizeof(d.dims));
+    memcpy(p.desc.periodic, d.periodic, sizeof(d.periodic));
+    memcpy(p.desc.rates, d.rates, sizeof(d.rates));
+    memcpy(p.desc.ubb_velocity, d.ubb_velocity, sizeof(d.ubb_velocity));
+    p.device = device;
+    p.q = common->stencil;
+    p.store = common->store_dtype;
+    p.partial = nullptr;
+    p.red_out = nullptr;
+    fill_physics(&p, &p.desc);
+}
+
+int64_t field_extent(const LbmDomainDesc& d, int q) {
+    const int64_t ex = d.dims[0] + 2, ey = d.dims[1] + 2, ez = d.dims[2] + 2;
+    return (q - 1) * d.strides[3] + (ez - 1) * d.strides[2] + (ey - 1) * d.strides[1] + ex;
+}
+
+int64_t flags_extent(const LbmDomainDesc& d) {
+    return int64_t(d.dims[0] + 2) * (d.dims[1] + 2) * (d.dims[2] + 2);
+}
+
+// Intervals [begin, end) must not overlap.
+bool disjoint(std::vector<std::pair<int64_t, int64_t>>& iv) {
+    std::sort(iv.begin(), iv.end());
+    for (size_t k = 1; k < iv.size(); ++k)
+        if (iv[k].first < iv[k - 1].second) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_batch_create(const LbmPlanDesc* common, const LbmDomainDesc* domains, int n_domains, void* buffer_a,
+                     void* buffer_b, int64_t buffer_elems, uint8_t* flags, int64_t flags_bytes,
+                     const LbmBatchTiling* tiling, LbmBatch** out) {
+    if (common == nullptr || domains == nullptr || tiling == nullptr || out == nullptr)
+        return fail(LBM_E_INVALID, "common, domains, tiling and out must not be NULL");
+    *out = nullptr;
+    if (n_domains < 1) return fail(LBM_E_INVALID, "a batch needs at least one domain");
+    const LbmBatchTiling t = *tiling;
+    if (t.tile_x < 1 || t.tile_y < 1 || t.tile_x * t.tile_y > 256 || t.cells_z < 1 || t.blocks_per_sm < 0)
+        return fail(LBM_E_INVALID, "tiling %dx%dx%d (%d blocks/SM): need tile_x*tile_y in [1, 256], cells_z >= 1",
+                    t.tile_x, t.tile_y, t.cells_z, t.blocks_per_sm);
+    if (common->pattern == LBM_PATTERN_ESOTWIST)
+        return fail(LBM_E_UNSUPPORTED, "batched sweeps are built for the pull and AA patterns");
+    const bool inplace = common->pattern != LBM_PATTERN_PULL;
+    if (inplace && buffer_b == nullptr) buffer_b = buffer_a;
+    if (inplace && buffer_b != buffer_a) return fail(LBM_E_INVALID, "in-place patterns use buffer_a only");
+    if (!inplace && buffer_a == buffer_b) return fail(LBM_E_INVALID, "the pull pattern needs two distinct buffers");
+
+    int device = -1;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    LbmPlan p0{};
+    domain_plan(common, domains[0], device, p0);
+    int rc;
+    if ((rc = check_device_ptr(&p0, buffer_a, "buffer_a", false))) return rc;
+    if ((rc = check_device_ptr(&p0, buffer_b, "buffer_b", false))) return rc;
+    if ((rc = check_device_ptr(&p0, flags, "flags", true))) return rc;
+
+    // Every domain on its own, then the batch as a whole.
+    bool all_cum1 = true;
+    std::vector<std::pair<int64_t, int64_t>> fields, flag_ranges;
+    int64_t cells = 0;
+    for (int k = 0; k < n_domains; ++k) {
+        const LbmDomainDesc& d = domains[k];
+        LbmPlan pk{};
+        domain_plan(common, d, device, pk);
+        if ((rc = validate_desc(&pk.desc))) return fail(rc, "domain %d: %s", k, g_err.c_str());
+        if ((rc = check_strides(&pk, d.strides))) return fail(rc, "domain %d: %s", k, g_err.c_str());
+        if (d.offset < 0 || d.offset + field_extent(d, pk.q) > buffer_elems)
+            return fail(LBM_E_INVALID, "domain %d: field at offset %lld runs past the %lld-element buffers", k,
+                        (long long)d.offset, (long long)buffer_elems);
+        fields.emplace_back(d.offset, d.offset + field_extent(d, pk.q));
+        if (d.flags_offset >= 0) {
+            if (flags == nullptr) return fail(LBM_E_INVALID, "domain %d has flags but the flag buffer is NULL", k);
+            if (d.flags_offset + flags_extent(d) > flags_bytes)
+                return fail(LBM_E_INVALID, "domain %d: flags at byte %lld run past the %lld-byte flag buffer", k,
+                            (long long)d.flags_offset, (long long)flags_bytes);
+            flag_ranges.emplace_back(d.flags_offset, d.flags_offset + flags_extent(d));
+        } else if (d.flags_offset != -1) {
+            return fail(LBM_E_INVALID, "domain %d: flags_offset must be >= 0 or -1", k);
+        }
+        if (!cumulant_high_orders_relax_to_equilibrium(&pk.desc)) all_cum1 = false;
+        cells += int64_t(d.dims[0]) * d.dims[1] * d.dims[2];
+    }
+    if (!disjoint(fields)) return fail(LBM_E_INVALID, "two domains' fields overlap");
+    if (!disjoint(flag_ranges)) return fail(LBM_E_INVALID, "two domains' flags overlap");
+
+    const int q = common->stencil;
+    int mk = common->method == LBM_METHOD_MRT ? MK_MRT : (common->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
+    if (mk == MK_CUM && all_cum1) mk = MK_CUM1;
+    const int store = common->store_dtype;
+    if (batched_launcher(q, mk, store, PAT_PULL) == nullptr)
+        return fail(LBM_E_UNSUPPORTED, "no batched kernel for this stencil/method/dtype");
+
+    // Per-domain arguments for both parities, and the tile table (domain-major, then z, y, x).
+    const size_t es = store_size(store);
+    char* A = static_cast<char*>(buffer_a);
+    char* B = static_cast<char*>(buffer_b);
+    std::vector<SweepArgs> args(2 * size_t(n_domains));
+    std::vector<BatchTile> tiles;
+    for (int k = 0; k < n_domains; ++k) {
+        const LbmDomainDesc& d = domains[k];
+        LbmPlan pk{};
+        domain_plan(common, d, device, pk);
+        SweepArgs a;
+        memset(&a, 0, sizeof(a));
+        a.g = make_grid(&pk, d.strides, d.flags_offset >= 0 ? flags + d.flags_offset : nullptr);
+        a.p = pk.phys;
+        a.omega_out = nullptr;
+        a.src = A + d.offset * es;
+        a.dst = B + d.offset * es;
+        args[k] = a;
+        a.src = B + d.offset * es;
+        a.dst = A + d.offset * es;
+        args[n_domains + k] = a;
+        for (int z = 0; z < d.dims[2]; z += t.cells_z)
+            for (int y = 0; y < d.dims[1]; y += t.tile_y)
+                for (int x = 0; x < d.dims[0]; x += t.tile_x) tiles.push_back(BatchTile{k, x, y, z});
+    }
+    if (tiles.size() >= (size_t(1) << 31)) return fail(LBM_E_INVALID, "too many tiles for one launch");
+
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    LbmBatch* b = new LbmBatch();
+    b->device = device;
+    b->q = q;
+    b->mk = mk;
+    b->store = store;
+    b->pattern = common->pattern;
+    b->n_domains = n_domains;
+    b->tiling = t;
+    b->n_tiles = (int64_t)tiles.size();
+    b->grid_blocks = t.blocks_per_sm == 0 ? b->n_tiles : std::min<int64_t>(b->n_tiles, int64_t(sms) * t.blocks_per_sm);
+    b->cells = cells;
+    b->d_domains = nullptr;
+    b->d_tiles = nullptr;
+    e = cudaMalloc(&b->d_domains, sizeof(SweepArgs) * args.size());
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, sizeof(BatchTile) * tiles.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_domains, args.data(), sizeof(SweepArgs) * args.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice);
+    // Near-wall marks, per domain with flags (as lbm_flags_finalize does for one field).
+    for (int k = 0; k < n_domains && e == cudaSuccess; ++k) {
+        if (domains[k].flags_offset < 0) continue;
+        const Grid& g = args[k].g;
+        const dim3 block(32, 8, 1), grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+        if (q == 19) k_flags_finalize<19><<<grid, block>>>(g);
+        else k_flags_finalize<27><<<grid, block>>>(g);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        cudaFree(b->d_domains);
+        cudaFree(b->d_tiles);
+        delete b;
+        return cuda_fail(e, "lbm_batch_create");
+    }
+    *out = b;
+    return LBM_OK;
+}
+
+int lbm_batch_sweep(const LbmBatch* b, int parity, void* stream) {
+    if (b == nullptr) return fail(LBM_E_INVALID, "batch is NULL");
+    if (parity != 0 && parity != 1) return fail(LBM_E_INVALID, "parity must be 0 (EVEN) or 1 (ODD)");
+    const bool inplace = b->pattern != LBM_PATTERN_PULL;
+    const int pat = inplace ? (parity ? PAT_AA_ODD : PAT_AA_EVEN) : PAT_PULL;
+    BatchLauncher L = batched_launcher(b->q, b->mk, b->store, pat);
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no batched kernel for this pattern");
+    BatchArgs a;
+    a.domains = b->d_domains;
+    a.tiles = b->d_tiles;
+    a.n_domains = b->n_domains;
+    a.n_tiles = (int)b->n_tiles;
+    a.cells_z = b->tiling.cells_z;
+    a.parity = inplace ? 0 : parity;
+    cudaError_t e = L(a, dim3((unsigned)b->grid_blocks), dim3(b->tiling.tile_x, b->tiling.tile_y, 1),
+                      static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "batched sweep launch");
+    return LBM_OK;
+}
+
+int lbm_batch_info(const LbmBatch* b, int64_t info[4]) {
+    if (b == nullptr || info == nullptr) return fail(LBM_E_INVALID, "batch and info must not be NULL");
+    info[0] = b->n_tiles;
+    info[1] = b->grid_blocks;
+    info[2] = b->cells;
+    info[3] = b->n_tiles * b->tiling.tile_x * b->tiling.tile_y * b->tiling.cells_z;
+    return LBM_OK;
+}
+
+int lbm_batch_destroy(LbmBatch* b) {
+    if (b == nullptr) return LBM_OK;
+    cudaFree(b->d_domains);
+    cudaFree(b->d_tiles);
+    delete b;
+    return LBM_OK;
 }
 
 }  // extern "C"

@@ -18,8 +18,9 @@ namespace lbm {
 
 // acc + c*x for a compile-time table coefficient c: zeros and unit factors fold away
 // (IEEE arithmetic forbids the compiler from dropping 0*x on its own).
-template <class R>
-__device__ __forceinline__ R cmad(R acc, double c, R x) {
+template <class R, class A>
+__device__ __forceinline__ R cmad(A acc_in, double c, R x) {
+    const R acc = acc_in;
     return c == 0.0 ? acc : (c == 1.0 ? acc + x : (c == -1.0 ? acc - x : acc + R(c) * x));
 }
 

@@ -2,7 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
-#include "lbm_kernels.cuh"
+#include "lbm_pair.cuh"
 
 namespace lbm {
 
@@ -19,6 +19,40 @@ template <class S, class R, int Q, int MK, int PAT>
 cudaError_t launch_set_eq(const MacroArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
     k_set_equilibrium<S, R, Q, MK, PAT><<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
+}
+
+template <class S, int Q, int MK, int PAT>
+cudaError_t launch_sweep_pair(const SweepArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
+    k_sweep_pair<S, Q, MK, PAT><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S, int Q, int MK>
+SweepLauncher pick_pair_pattern(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_sweep_pair<S, Q, MK, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_sweep_pair<S, Q, MK, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_sweep_pair<S, Q, MK, PAT_AA_ODD>;
+    }
+    return nullptr;
+}
+
+using BatchLauncher = cudaError_t (*)(const BatchArgs&, dim3, dim3, cudaStream_t);
+
+template <class S, class R, int Q, int MK, int PAT>
+cudaError_t launch_batched(const BatchArgs& b, dim3 grid, dim3 block, cudaStream_t s) {
+    k_sweep_batched<S, R, Q, MK, PAT><<<grid, block, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+template <class S, class R, int Q, int MK>
+BatchLauncher pick_batched_pattern(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_batched<S, R, Q, MK, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_batched<S, R, Q, MK, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_batched<S, R, Q, MK, PAT_AA_ODD>;
+    }
+    return nullptr;
 }
 
 template <class S, class R, int Q, int MK>
@@ -58,6 +92,19 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         }                                                                                       \
         return nullptr;                                                                         \
     }                                                                                           \
+    BatchLauncher batched_##NAME(int store, int pat) {                                          \
+        if (store == ST_F64) return pick_batched_pattern<double, double, Q, MK>(pat);           \
+        if (store == ST_F32) return pick_batched_pattern<float, float, Q, MK>(pat);             \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
+        switch (store) {                                                                        \
+            case ST_F32: return pick_pair_pattern<float, Q, MK>(pat);                            \
+            case ST_F16: return pick_pair_pattern<__half, Q, MK>(pat);                           \
+            case ST_BF16: return pick_pair_pattern<__nv_bfloat16, Q, MK>(pat);                  \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }                                                                                           \
     MacroLauncher set_eq_##NAME(int store, int pat) {                                           \
         switch (store) {                                                                        \
             case ST_F64: return pick_set_eq_pattern<double, double, Q, MK>(pat);                 \
@@ -89,6 +136,14 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         }                                                                                       \
         return nullptr;                                                                         \
     }                                                                                           \
+    BatchLauncher batched_##NAME(int store, int pat) {                                          \
+        if (store == ST_F32) return pick_batched_pattern<float, float, Q, MK>(pat);             \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
+        if (store == ST_F32) return pick_pair_pattern<float, Q, MK>(pat);                       \
+        return nullptr;                                                                         \
+    }                                                                                           \
     SweepLauncher sweep_##NAME(int store, int pat) {                                            \
         if (store == ST_F64) return NAME##_sweep_pat<double, double>(pat);                      \
         if (store == ST_F32) return NAME##_sweep_pat<float, float>(pat);                        \
@@ -100,8 +155,10 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         return nullptr;                                                                         \
     }
 
-#define LBM_DECLARE_FAMILY(NAME)                   \
-    SweepLauncher sweep_##NAME(int store, int pat); \
+#define LBM_DECLARE_FAMILY(NAME)                        \
+    BatchLauncher batched_##NAME(int store, int pat);    \
+    SweepLauncher sweep_##NAME(int store, int pat);      \
+    SweepLauncher sweep_pair_##NAME(int store, int pat); \
     MacroLauncher set_eq_##NAME(int store, int pat);
 
 LBM_DECLARE_FAMILY(q19_pop)

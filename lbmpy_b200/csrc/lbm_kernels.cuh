@@ -111,15 +111,12 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
     }
 }
 
+// The whole update of one cell: pull through the accessor, fused bounce-back, collision, push
+// through the accessor.  Shared by the single-domain and the batched sweeps.
 template <class S, class R, int Q, int MK, int PAT>
-__global__ void __launch_bounds__(256) k_sweep(const SweepArgs a) {
-    using L = Lat<Q>;
+__device__ __forceinline__ void sweep_cell(const SweepArgs& a, int x, int y, int z) {
     using A = Access<PAT>;
     const Grid& g = a.g;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    if (x >= g.nx || y >= g.ny) return;
     int fl = 0;
     if (g.flags != nullptr) {
         fl = g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz];
@@ -144,6 +141,61 @@ __global__ void __launch_bounds__(256) k_sweep(const SweepArgs a) {
         Conv<S, R>::st(dst + eidx(A::template wslot<Q>(i) * g.sq, cell + off), f[i]);
     }
     if (a.omega_out != nullptr) a.omega_out[x + g.nx * (y + (long long)g.ny * z)] = (float)om;
+}
+
+template <class S, class R, int Q, int MK, int PAT>
+__global__ void __launch_bounds__(256) k_sweep(const SweepArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= a.g.nx || y >= a.g.ny) return;
+    sweep_cell<S, R, Q, MK, PAT>(a, x, y, z);
+}
+
+// ------------------------------------------------------------------ batched domains
+// Many independent domains (each with its own ghost layers, strides, flags and rates) updated by
+// one persistent launch: the blocks walk a table of tiles, each tile_x x tile_y cells of
+// `cells_z` consecutive x-y planes of one domain (a thread updates up to cells_z cells along z).
+// Each domain carries a full SweepArgs whose pointers already point into the shared source and
+// destination buffers of the batch, one set per step parity.  A block stages the arguments of
+// its current domain in shared memory, so the collision reads its rates from there.
+struct BatchTile {
+    int domain, x0, y0, z0;
+};
+
+struct BatchArgs {
+    const SweepArgs* domains;     // device array, [parity][n_domains]
+    const BatchTile* tiles;       // device array
+    int n_domains, n_tiles;
+    int cells_z;
+    int parity;                   // selects which half of `domains` (src/dst swapped) to use
+};
+
+template <class S, class R, int Q, int MK, int PAT>
+__global__ void __launch_bounds__(256) k_sweep_batched(const BatchArgs b) {
+    __shared__ __align__(16) SweepArgs sa;
+    constexpr int WORDS = sizeof(SweepArgs) / 4;
+    static_assert(sizeof(SweepArgs) % 4 == 0, "SweepArgs is copied as 32-bit words");
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nthreads = blockDim.x * blockDim.y;
+    int staged = -1;
+    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
+        const BatchTile tile = b.tiles[t];
+        if (tile.domain != staged) {
+            __syncthreads();                         // every thread is done with the previous domain
+            const unsigned* from = reinterpret_cast<const unsigned*>(b.domains + b.parity * b.n_domains + tile.domain);
+            unsigned* to = reinterpret_cast<unsigned*>(&sa);
+            for (int w = tid; w < WORDS; w += nthreads) to[w] = from[w];
+            __syncthreads();
+            staged = tile.domain;
+        }
+        const int x = tile.x0 + threadIdx.x;
+        const int y = tile.y0 + threadIdx.y;
+        if (x < sa.g.nx && y < sa.g.ny) {
+            const int z1 = min(tile.z0 + b.cells_z, sa.g.nz);
+            for (int z = tile.z0; z < z1; ++z) sweep_cell<S, R, Q, MK, PAT>(sa, x, y, z);
+        }
+    }
 }
 
 // ------------------------------------------------------------------ setter / getter

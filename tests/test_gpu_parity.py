@@ -117,9 +117,12 @@ def _boundaries(kind):
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("dtype", ["float64", "float32"])
-def test_sweep_parity(cuda, case, dtype):
+@pytest.mark.parametrize("dtype,kernel", [("float64", "cell"), ("float32", "pair"), ("float32", "cell")])
+def test_sweep_parity(cuda, case, dtype, kernel, monkeypatch):
+    """kernel='pair': two cells per thread with packed FP32x2 arithmetic (the default for even nx);
+    kernel='cell': one cell per thread (forced with LBM_B200_PAIR=0)."""
     name, stencil, method, pattern, n, periodic, bkind, kw = case
+    monkeypatch.setenv("LBM_B200_PAIR", "1" if kernel == "pair" else "0")
     if dtype == "float32" and stencil == "D3Q27" and method == "mrt" and pattern not in ("pull", "aa"):
         pytest.skip("not built")
     steps = 100
@@ -147,9 +150,11 @@ def test_sweep_parity(cuda, case, dtype):
 
 
 @pytest.mark.parametrize("storage,bound", [("float16", 1e-3), ("bfloat16", 5e-3)])
-def test_low_precision_storage_l2_velocity(cuda, storage, bound):
+@pytest.mark.parametrize("kernel", ["pair", "cell"])
+def test_low_precision_storage_l2_velocity(cuda, storage, bound, kernel, monkeypatch):
     """Zero-centred 16-bit storage with FP32 collision vs the FP64 oracle (TGV + noise).
     FP16 meets the 1e-3 bar; BF16's 8-bit mantissa leaves a few 1e-3 (bound stated per type)."""
+    monkeypatch.setenv("LBM_B200_PAIR", "1" if kernel == "pair" else "0")
     n = (32, 32, 16)
     u = tgv_velocity(n, 0.04, noise=1e-3, seed=0)
     rho = np.ones(n)

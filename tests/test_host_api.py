@@ -37,6 +37,33 @@ def test_plan_descriptor_layout_matches_header():
     assert ctypes.sizeof(N.LbmPlanDesc) % 8 == 0
 
 
+def test_batch_descriptor_layout_and_host_checks():
+    """LbmDomainDesc / LbmBatchTiling match the header; arguments that need no device are refused
+    before any CUDA call."""
+    assert N.LbmDomainDesc.strides.offset == 24
+    assert N.LbmDomainDesc.rates.offset == 72
+    assert N.LbmDomainDesc.ubb_velocity.offset == 72 + 27 * 8
+    assert ctypes.sizeof(N.LbmDomainDesc) == 72 + 27 * 8 + 12 * 8
+    assert ctypes.sizeof(N.LbmBatchTiling) == 16
+    common = N.LbmPlanDesc()
+    common.stencil = 19
+    doms = (N.LbmDomainDesc * 1)()
+    h = ctypes.c_void_p()
+
+    def create(n, tiling):
+        t = N.LbmBatchTiling(*tiling)
+        return N.lib().lbm_batch_create(ctypes.byref(common), doms, n, None, None, 0, None, 0, ctypes.byref(t),
+                                        ctypes.byref(h))
+    assert create(0, (32, 8, 1, 0)) == N.LBM_E_INVALID
+    assert create(1, (32, 16, 1, 0)) == N.LBM_E_INVALID
+    assert create(1, (32, 8, 0, 0)) == N.LBM_E_INVALID
+    assert "tiling" in N.last_error()
+    common.pattern = N.PATTERN_ESOTWIST
+    assert create(1, (32, 8, 1, 0)) == N.LBM_E_UNSUPPORTED
+    assert N.lib().lbm_batch_sweep(None, 0, None) == N.LBM_E_INVALID
+    assert N.lib().lbm_batch_destroy(None) == N.LBM_OK
+
+
 def test_trt_magic_number_and_delta_equilibrium():
     cfg = L.LBMConfig(stencil=L.Stencil.D3Q19, method=L.Method.TRT, relaxation_rate=1.8)
     assert cfg.relaxation_rates[1] == pytest.approx(0.25806451612903225)
