@@ -33,6 +33,15 @@ FORCE = 1e-7
 E2E_SWEEPS = 100          # sweeps per end-to-end call (one LatticeBoltzmannStep.run() in lbmpy terms)
 FALLBACK_HBM_GBS = 6650.0
 
+# DRAM bytes (read + write) per sweep launch from one ncu capture of the same workload, averaged
+# over the launches captured; summaries with their commands are under profiles/.
+NCU_TRAFFIC_BYTES = {
+    "d3q27-cumulant-aa-channel-256x128x128": 876_794_112,   # k_sweep_d3q27_cumulant_aa_channel_256x128x128.md
+    "d3q19-trt-pull-float32-256": 2_547_412_000,            # k_sweep_d3q19_fp32_fp16_256.md
+    "d3q19-mrt-pull-float32-256": 2_550_143_000,
+    "d3q19-trt-pull-float16-256": 1_279_790_080,
+}
+
 
 def algorithmic_bytes_per_sweep(cells: int, q: int = Q, itemsize: int = 4) -> int:
     """2 * Q * sizeof(PDF) per lattice update: every population read once and written once."""
@@ -133,8 +142,8 @@ for _n in (64, 256, 512):
 
 
 def make_cavity_batch(device, n_cavities=512, seed=0):
-    """512 independent lid-driven cavities (D3Q19 MRT, FP32, pull), edges seeded from
-    {16, 24, ..., 96} per axis, shear/bulk rates seeded uniform in [1.5, 1.95], lid 0.05; one
+    """512 independent cubic lid-driven cavities (D3Q19 MRT, FP32, pull), edge seeded from
+    {16, 24, ..., 96}, shear/bulk rates seeded uniform in [1.5, 1.95], lid 0.05; one
     persistent launch per step over all cavities, tiling autotuned, steps replayed from a CUDA
     graph."""
     from lbmpy_b200.batched import lid_driven_cavity_batch
@@ -291,11 +300,7 @@ def main():
     # roofline of the sweep kernel (the only kernel in the timed region)
     peak, peak_kind = measured_peak()
     achieved = algorithmic_bytes_per_sweep(cells, q_pop, itemsize) / (ms / args.steps * 1e-3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "sweep_traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as fh:
-            traffic = json.load(fh).get("d3q27_cumulant_aa_channel_fp32_bytes_per_launch")
+    traffic = NCU_TRAFFIC_BYTES.get(args.workload)
 
     # end to end through the public API: host PDFs in, run, PDFs and macroscopic fields out
     e2e = None

@@ -43,7 +43,7 @@ enum { LBM_DTYPE_F64 = 0, LBM_DTYPE_F32 = 1, LBM_DTYPE_F16 = 2, LBM_DTYPE_BF16 =
 enum { LBM_PATTERN_PULL = 0, LBM_PATTERN_AA = 1, LBM_PATTERN_ESOTWIST = 2 };
 enum { LBM_FORCE_NONE = 0, LBM_FORCE_GUO = 1, LBM_FORCE_CENTRAL_MOMENT = 2, LBM_FORCE_SIMPLE = 3,
        LBM_FORCE_LUO = 4 };
-enum { LBM_SGS_NONE = 0, LBM_SGS_SMAGORINSKY = 1 };
+enum { LBM_SGS_NONE = 0, LBM_SGS_SMAGORINSKY = 1, LBM_SGS_MLP = 2 };
 
 /* Everything a sweep needs, resolved on the host by the lbmpy-compatible front end
  * (LBMConfig.__post_init__, creationfunctions.py:347-484, and create_lb_method, :773-868). */
@@ -130,6 +130,34 @@ int lbm_reduce_conserved_noalloc(const LbmPlanDesc* desc, const void* pdfs, cons
  * neighbour along the plan's stencil, honouring periodicity.  Replaces the link-list setup of
  * LatticeBoltzmannBoundaryHandling (boundaries/boundaryhandling.py:15-155). */
 int lbm_flags_finalize(const LbmPlan* plan, uint8_t* flags, void* stream);
+
+/* ---- Learned eddy-viscosity closure ----
+ * sgs = LBM_SGS_MLP replaces the closed-form eddy viscosity of lbmpy's Smagorinsky model
+ * (turbulence_models.py:25-84: omega = 2 / (tau0 + sqrt(18 C^2 Pi + tau0^2))) by a 10-32-32-1
+ * perceptron evaluated per cell inside the D3Q27 cumulant sweep: omega = 1 / (tau0 + 3 nu_t) on
+ * the moments in sgs_mask.  No lbmpy counterpart beyond that hook.  Parameter block: 1442 FP32
+ * values, W1[10][32] b1[32] W2[32][32] b2[32] W3[32] b3 scale (nu_t = scale * softplus(y)). */
+
+/* Uploads the parameters (host memory) that every closure sweep on the current device reads;
+ * one set per device and process, ordered on `stream` before later launches. */
+int lbm_closure_set_weights(const float* params, int n, void* stream);
+/* Features of n cells from their state, SoA [10][n] device arrays: Pi_xx Pi_yy Pi_zz Pi_xy
+ * Pi_xz Pi_yz (pre-collision non-equilibrium stress), rho, ux, uy, uz -> feats [10][n]. */
+int lbm_closure_features(const float* state, int64_t n, float* feats, void* stream);
+/* nu_t of n samples (feats [10][n]) with device parameters `params`. */
+int lbm_mlp_forward(const float* params, const float* feats, int64_t n, float* nu, void* stream);
+
+typedef struct LbmMlp LbmMlp;
+/* Trainer state: partial-gradient scratch for up to max_blocks blocks. */
+int lbm_mlp_create(int max_blocks, LbmMlp** out);
+int lbm_mlp_destroy(LbmMlp* trainer);
+/* loss = sum_n w_n (nu_n - t_n)^2 * inv_wsum and its gradient (1442 floats, the scale entry 0);
+ * weight may be NULL (all 1); loss (one double, device) may be NULL.  Deterministic. */
+int lbm_mlp_loss_grad(LbmMlp* trainer, const float* params, const float* feats, const float* target,
+                      const float* weight, int64_t n, double inv_wsum, float* grad, double* loss, void* stream);
+/* One Adam step (bias-corrected, step counts from 1) on the trained parameters, in place. */
+int lbm_mlp_adam(const float* grad, float* params, float* m1, float* m2, double lr, double beta1, double beta2,
+                 double eps, int step, void* stream);
 
 /* ---- Batched domains: many independent fields of uneven size in one persistent launch ----
  * No single lbmpy counterpart: lbmpy runs one LatticeBoltzmannStep (lbstep.py:18-450) per

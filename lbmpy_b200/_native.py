@@ -16,12 +16,14 @@ METHOD_SRT, METHOD_TRT, METHOD_MRT, METHOD_CUMULANT = 0, 1, 2, 3
 DTYPE_F64, DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2, 3
 PATTERN_PULL, PATTERN_AA, PATTERN_ESOTWIST = 0, 1, 2
 FORCE_NONE, FORCE_GUO, FORCE_CENTRAL_MOMENT, FORCE_SIMPLE, FORCE_LUO = 0, 1, 2, 3, 4
-SGS_NONE, SGS_SMAGORINSKY = 0, 1
+SGS_NONE, SGS_SMAGORINSKY, SGS_MLP = 0, 1, 2
+MLP_PARAMS = 1442
 
 # exported symbols, one per declaration in include/lbm_b200.h
 EXPORTS = ("lbm_plan_create", "lbm_plan_destroy", "lbm_plan_update", "lbm_sweep", "lbm_run",
            "lbm_set_equilibrium", "lbm_get_macroscopic", "lbm_reduce_conserved", "lbm_reduce_conserved_noalloc",
-           "lbm_flags_finalize", "lbm_batch_create", "lbm_batch_sweep", "lbm_batch_info", "lbm_batch_destroy",
+           "lbm_flags_finalize", "lbm_closure_set_weights", "lbm_closure_features", "lbm_mlp_forward",
+           "lbm_mlp_create", "lbm_mlp_destroy", "lbm_mlp_loss_grad", "lbm_mlp_adam", "lbm_batch_create", "lbm_batch_sweep", "lbm_batch_info", "lbm_batch_destroy",
            "lbm_last_error", "lbm_version")
 
 
@@ -84,6 +86,14 @@ def lib():
         L.lbm_reduce_conserved_noalloc.argtypes = [ctypes.POINTER(LbmPlanDesc), vp, i64p, vp, ctypes.c_int,
                                                    ctypes.POINTER(ctypes.c_double), vp]
         L.lbm_flags_finalize.argtypes = [vp, vp, vp]
+        L.lbm_closure_set_weights.argtypes = [vp, ctypes.c_int, vp]
+        L.lbm_closure_features.argtypes = [vp, ctypes.c_int64, vp, vp]
+        L.lbm_mlp_forward.argtypes = [vp, vp, ctypes.c_int64, vp, vp]
+        L.lbm_mlp_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.lbm_mlp_destroy.argtypes = [vp]
+        L.lbm_mlp_loss_grad.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int64, ctypes.c_double, vp, vp, vp]
+        L.lbm_mlp_adam.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_int, vp]
         L.lbm_batch_create.argtypes = [ctypes.POINTER(LbmPlanDesc), ctypes.POINTER(LbmDomainDesc), ctypes.c_int, vp,
                                        vp, ctypes.c_int64, vp, ctypes.c_int64, ctypes.POINTER(LbmBatchTiling),
                                        ctypes.POINTER(ctypes.c_void_p)]

@@ -382,18 +382,20 @@ class LatticeBoltzmannBatch:
 
 
 def lid_driven_cavity_batch(n_cavities: int, seed: int = 0, edges=tuple(range(16, 97, 8)), lid_velocity=0.05,
-                            omega_range=(1.5, 1.95), storage_dtype="float32", **kwargs) -> LatticeBoltzmannBatch:
+                            omega_range=(1.5, 1.95), storage_dtype="float32", cubic=True,
+                            **kwargs) -> LatticeBoltzmannBatch:
     """A batch of independent lid-driven cavities (lbmpy ``create_lid_driven_cavity``,
     ``scenarios.py:72-101``: UBB lid on the N face moving in x, NoSlip on W, E, S, T, B) with the
-    D3Q19 weighted-orthogonal MRT method.  Per cavity, seeded: edge lengths drawn from `edges`
-    independently per axis, shear and bulk rates drawn uniformly from `omega_range`; the higher
-    moments relax with rate 1."""
+    D3Q19 weighted-orthogonal MRT method.  Per cavity, seeded: the edge length drawn from `edges`
+    (one edge per cube, or one per axis with cubic=False), shear and bulk rates drawn uniformly
+    from `omega_range`; the higher moments relax with rate 1."""
     import sympy as sp
     from .boundaries import NoSlip, UBB, slice_from_direction
     from .creationfunctions import CreateKernelConfig, LBMConfig, LBMOptimisation
     from .enums import Method
     rng = np.random.default_rng(seed)
-    sizes = [tuple(int(e) for e in rng.choice(edges, 3)) for _ in range(n_cavities)]
+    sizes = [tuple(int(e) for e in rng.choice(edges, 1 if cubic else 3)) * (3 if cubic else 1)
+             for _ in range(n_cavities)]
     rates = rng.uniform(omega_range[0], omega_range[1], size=(n_cavities, 2))
     w_s, w_b = sp.Symbol("omega_shear"), sp.Symbol("omega_bulk")
     cfg = LBMConfig(stencil=LBStencil(Stencil.D3Q19), method=Method.MRT, relaxation_rates=[w_s, w_b, 1, 1],

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liblbmb200.so")
 SOURCES = ["lbm_abi.cu", "lbm_q19_pop.cu", "lbm_q19_mrt.cu", "lbm_q27_pop.cu", "lbm_q27_mrt.cu",
-           "lbm_q27_cum.cu", "lbm_q27_cum1.cu"]
+           "lbm_q27_cum.cu", "lbm_q27_cum1.cu", "lbm_q27_closure.cu", "lbm_mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -43,13 +43,36 @@ def flags(verbose=False) -> list:
     return f
 
 
+def _includes(name: str, seen: set) -> None:
+    """Quoted includes of a csrc file, transitively."""
+    if name in seen:
+        return
+    path = os.path.join(CSRC, name)
+    if not os.path.exists(path):
+        return
+    seen.add(name)
+    with open(path) as fh:
+        for line in fh:
+            line = line.strip()
+            if line.startswith("#include \""):
+                inc = line.split('"')[1]
+                if "/" not in inc:
+                    _includes(inc, seen)
+
+
 def _digest(source: str = None) -> str:
-    """Hash of the shared headers, the compiler flags and one source (or all sources)."""
+    """Hash of the compiler flags, the public header and the given source with every csrc header
+    it includes (or of all sources and headers)."""
     h = hashlib.sha256()
-    for name in sorted(os.listdir(CSRC)):
-        if name.endswith((".cuh", ".h")) or (name.endswith(".cu") and (source is None or name == source)):
-            with open(os.path.join(CSRC, name), "rb") as fh:
-                h.update(name.encode() + fh.read())
+    if source is None:
+        names = sorted(n for n in os.listdir(CSRC) if n.endswith((".cuh", ".h", ".cu")))
+    else:
+        seen = set()
+        _includes(source, seen)
+        names = sorted(seen)
+    for name in names:
+        with open(os.path.join(CSRC, name), "rb") as fh:
+            h.update(name.encode() + fh.read())
     with open(os.path.join(HERE, "..", "include", "lbm_b200.h"), "rb") as fh:
         h.update(fh.read())
     h.update(" ".join(flags()).encode())

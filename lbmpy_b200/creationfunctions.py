@@ -370,6 +370,7 @@ class LbmCollisionRule:
     subgrid_scale_model: Any = None
     smagorinsky_constant: float = 0.12
     output: dict = field(default_factory=dict)
+    closure: Any = None               # MLPClosure for SubgridScaleModel.LEARNED
     simplification_hints: dict = field(default_factory=dict)
 
 
@@ -385,14 +386,24 @@ def create_lb_collision_rule(lb_method=None, lbm_config=None, lbm_optimisation=N
         raise NotImplementedError("density/velocity input fields are not built")
     if lbm_config.galilean_correction and (lb_method.kind != "cumulant" or lb_method.stencil.name != "D3Q27"):
         raise ValueError("Galilean correction is only defined for D3Q27 cumulant methods.")
-    sgs, c = None, 0.12
+    sgs, c, closure = None, 0.12, None
     if lbm_config.subgrid_scale_model:
         sgs = lbm_config.subgrid_scale_model
         if isinstance(sgs, tuple):
-            sgs, c = sgs[0], float(sgs[1])
-        if sgs != SubgridScaleModel.SMAGORINSKY:
-            raise NotImplementedError("only the Smagorinsky subgrid-scale model is built")
-    rule = LbmCollisionRule(lb_method, bool(lbm_config.galilean_correction), sgs, c, dict(lbm_config.output))
+            sgs, arg = sgs[0], sgs[1]
+            if sgs == SubgridScaleModel.LEARNED:
+                closure = arg
+            else:
+                c = float(arg)
+        if sgs == SubgridScaleModel.LEARNED:
+            if closure is None:
+                raise ValueError("the learned closure needs its network: (SubgridScaleModel.LEARNED, MLPClosure)")
+            if lb_method.kind != "cumulant" or lb_method.stencil.name != "D3Q27":
+                raise NotImplementedError("the learned closure is built for the D3Q27 cumulant method")
+        elif sgs != SubgridScaleModel.SMAGORINSKY:
+            raise NotImplementedError("the Smagorinsky and learned subgrid-scale models are built")
+    rule = LbmCollisionRule(lb_method, bool(lbm_config.galilean_correction), sgs, c, dict(lbm_config.output),
+                            closure=closure)
     lbm_config.collision_rule = rule
     return rule
 

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/lbm_b200.h"
+#include "lbm_closure.cuh"
 #include "lbm_dispatch.h"
 
 using namespace lbm;
@@ -105,9 +106,14 @@ Grid make_grid(const LbmPlan* p, const int64_t s[4], const uint8_t* flags) {
     return g;
 }
 
+// 256-thread blocks shaped along x: the widest of 128 / 64 / 32 threads whose last block in a
+// row idles at most 1/8 of the row (else 32).
 void launch_shape(const Grid& g, dim3& grid, dim3& block) {
     int bx = 32;
-    while (bx < g.nx && bx < 128) bx *= 2;
+    for (int c : {128, 64}) {
+        const int waste = (g.nx + c - 1) / c * c - g.nx;
+        if (c <= 2 * g.nx && 8 * waste <= g.nx) { bx = c; break; }
+    }
     const int by = 256 / bx;
     block = dim3(bx, by, 1);
     grid = dim3((g.nx + bx - 1) / bx, (g.ny + by - 1) / by, g.nz);
@@ -129,6 +135,7 @@ SweepLauncher sweep_launcher(const LbmPlan* p, int pat) {
     if (p->q == 27 && p->mk == MK_MRT) return sweep_q27_mrt(p->store, pat);
     if (p->q == 27 && p->mk == MK_CUM) return sweep_q27_cum(p->store, pat);
     if (p->q == 27 && p->mk == MK_CUM1) return sweep_q27_cum1(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM1_MLP) return sweep_q27_closure(p->store, pat);
     return nullptr;
 }
 
@@ -172,7 +179,8 @@ MacroLauncher set_eq_launcher(const LbmPlan* p, int pat) {
     if (p->q == 19 && p->mk == MK_MRT) return set_eq_q19_mrt(p->store, pat);
     if (p->q == 27 && p->mk == MK_POP) return set_eq_q27_pop(p->store, pat);
     if (p->q == 27 && p->mk == MK_MRT) return set_eq_q27_mrt(p->store, pat);
-    if (p->q == 27 && (p->mk == MK_CUM || p->mk == MK_CUM1)) return set_eq_q27_cum(p->store, pat);
+    if (p->q == 27 && (p->mk == MK_CUM || p->mk == MK_CUM1 || p->mk == MK_CUM1_MLP))
+        return set_eq_q27_cum(p->store, pat);
     return nullptr;
 }
 
@@ -292,6 +300,13 @@ bool cumulant_high_orders_relax_to_equilibrium(const LbmPlanDesc* d) {
     return true;
 }
 
+int method_kind(const LbmPlanDesc* d) {
+    if (d->method == LBM_METHOD_MRT) return MK_MRT;
+    if (d->method != LBM_METHOD_CUMULANT) return MK_POP;
+    if (!cumulant_high_orders_relax_to_equilibrium(d)) return MK_CUM;
+    return d->sgs == LBM_SGS_MLP ? MK_CUM1_MLP : MK_CUM1;
+}
+
 int validate_desc(const LbmPlanDesc* d) {
     if (d->stencil != 19 && d->stencil != 27) return fail(LBM_E_UNSUPPORTED, "stencil must be D3Q19 or D3Q27");
     if (d->method < 0 || d->method > 3) return fail(LBM_E_INVALID, "unknown method %d", d->method);
@@ -309,9 +324,18 @@ int validate_desc(const LbmPlanDesc* d) {
         return fail(LBM_E_INVALID, "This force model can only be combined with the Cumulant collision model");
     if (d->galilean_correction && d->method != LBM_METHOD_CUMULANT)
         return fail(LBM_E_INVALID, "Galilean correction is only defined for D3Q27 cumulant methods.");
-    if (d->sgs != LBM_SGS_NONE && d->sgs != LBM_SGS_SMAGORINSKY) return fail(LBM_E_INVALID, "unknown SGS model");
-    if (d->sgs == LBM_SGS_SMAGORINSKY && !(d->shear_rate > 0.0))
-        return fail(LBM_E_INVALID, "the Smagorinsky model needs a positive shear relaxation rate");
+    if (d->sgs != LBM_SGS_NONE && d->sgs != LBM_SGS_SMAGORINSKY && d->sgs != LBM_SGS_MLP)
+        return fail(LBM_E_INVALID, "unknown SGS model");
+    if (d->sgs != LBM_SGS_NONE && !(d->shear_rate > 0.0))
+        return fail(LBM_E_INVALID, "a subgrid-scale model needs a positive shear relaxation rate");
+    if (d->sgs == LBM_SGS_MLP &&
+        (d->method != LBM_METHOD_CUMULANT || d->stencil != 27 || !cumulant_high_orders_relax_to_equilibrium(d)))
+        return fail(LBM_E_UNSUPPORTED,
+                    "the learned closure is built for the D3Q27 cumulant method with orders >= 3 relaxed by 1");
+    if (d->sgs == LBM_SGS_MLP && d->store_dtype != LBM_DTYPE_F32 && d->store_dtype != LBM_DTYPE_F64)
+        return fail(LBM_E_UNSUPPORTED, "the learned closure is built for FP32 and FP64 storage");
+    if (d->sgs == LBM_SGS_MLP && d->pattern == LBM_PATTERN_ESOTWIST)
+        return fail(LBM_E_UNSUPPORTED, "the learned closure is built for the pull and AA patterns");
     for (int k = 0; k < 3; ++k)
         if (d->dims[k] < 1) return fail(LBM_E_INVALID, "dims must be positive, got %d in axis %d", d->dims[k], k);
     if (d->dims[1] > 65535 * 8 || d->dims[2] > 65535)
@@ -320,6 +344,16 @@ int validate_desc(const LbmPlanDesc* d) {
 }
 
 }  // namespace
+
+int lbm::abi_fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
 
 extern "C" {
 
@@ -341,8 +375,7 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
     cudaError_t e = cudaGetDevice(&p->device);
     if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaGetDevice"); }
     p->q = desc->stencil;
-    p->mk = desc->method == LBM_METHOD_MRT ? MK_MRT : (desc->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
-    if (p->mk == MK_CUM && cumulant_high_orders_relax_to_equilibrium(desc)) p->mk = MK_CUM1;
+    p->mk = method_kind(desc);
     p->store = desc->store_dtype;
     {
         const char* env = getenv("LBM_B200_PAIR");
@@ -373,8 +406,7 @@ int lbm_plan_update(LbmPlan* p, const LbmPlanDesc* desc) {
     int rc = validate_desc(desc);
     if (rc) return rc;
     p->desc = *desc;
-    p->mk = desc->method == LBM_METHOD_MRT ? MK_MRT : (desc->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
-    if (p->mk == MK_CUM && cumulant_high_orders_relax_to_equilibrium(desc)) p->mk = MK_CUM1;
+    p->mk = method_kind(desc);
     fill_physics(p, desc);
     return LBM_OK;
 }
@@ -532,6 +564,18 @@ int lbm_reduce_conserved(const LbmPlan* p, const void* pdfs, const int64_t strid
     return e == cudaSuccess ? LBM_OK : cuda_fail(e, "reduction sync");
 }
 
+int lbm_closure_set_weights(const float* params, int n, void* stream) {
+    if (params == nullptr) return fail(LBM_E_INVALID, "params is NULL");
+    if (n != MLP_PARAMS) return fail(LBM_E_INVALID, "the closure takes %d parameters, got %d", MLP_PARAMS, n);
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, params) == cudaSuccess && at.type == cudaMemoryTypeDevice)
+        return fail(LBM_E_INVALID, "params must be host memory");
+    cudaGetLastError();
+    cudaError_t e = closure_upload(params, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "closure upload");
+    return LBM_OK;
+}
+
 int lbm_flags_finalize(const LbmPlan* p, uint8_t* flags, void* stream) {
     if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
     int rc;
@@ -669,6 +713,7 @@ int lbm_batch_create(const LbmPlanDesc* common, const LbmDomainDesc* domains, in
     if (!disjoint(flag_ranges)) return fail(LBM_E_INVALID, "two domains' flags overlap");
 
     const int q = common->stencil;
+    if (common->sgs == LBM_SGS_MLP) return fail(LBM_E_UNSUPPORTED, "batched sweeps do not take the learned closure");
     int mk = common->method == LBM_METHOD_MRT ? MK_MRT : (common->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
     if (mk == MK_CUM && all_cum1) mk = MK_CUM1;
     const int store = common->store_dtype;

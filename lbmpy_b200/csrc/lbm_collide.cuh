@@ -401,8 +401,12 @@ __device__ __forceinline__ R collide_cum(R (&f)[27], const Physics& p) {
 // central moments are formed directly as deviations from the central moments of the lattice-weight
 // background, Delta = kappa* - B(u) (B separable: B0 = 1, B1 = -u, B2 = 1/3 + u^2); the inverse
 // transform of Delta gives the zero-centred populations with no O(1/3) cancellation.
-template <class R>
-__device__ __forceinline__ R collide_cum_ho1(R (&f)[27], const Physics& p) {
+//
+// CLOSURE: the shear rate comes from an eddy viscosity nu_t(Pi_xx, Pi_yy, Pi_zz, Pi_xy, Pi_xz,
+// Pi_yz, rho, ux, uy, uz) evaluated on the same non-equilibrium stress the Smagorinsky branch uses
+// (the learned closure, lbm_closure.cuh), as omega = 1 / (tau0 + 3 nu_t).
+template <class R, bool CLOSURE = false, class NU = int>
+__device__ __forceinline__ R collide_cum_ho1(R (&f)[27], const Physics& p, const NU& nu_t = NU()) {
     // raw moments of f~ (no shift) on the velocity cube: m[a*9 + b*3 + c]
     R m[27];
 #pragma unroll
@@ -450,7 +454,7 @@ __device__ __forceinline__ R collide_cum_ho1(R (&f)[27], const Physics& p) {
     const R k011 = M_(0, 1, 1) - uy * M_(0, 0, 1) - uz * M_(0, 1, 0) + uy * uz * drho + uy * uz;
 #undef M_
     R om_sgs = R(0);
-    if (p.sgs == 1) {
+    if (CLOSURE || p.sgs == 1) {
         // Pi_neq from the central moments: raw second moments minus their equilibrium values
         const R pxx = a0 - ux * R(p.force[0]) * R(cm_force ? 1 : 0);
         const R pyy = b0 - uy * R(p.force[1]) * R(cm_force ? 1 : 0);
@@ -459,14 +463,18 @@ __device__ __forceinline__ R collide_cum_ho1(R (&f)[27], const Physics& p) {
         const R fxz = cm_force ? R(0.5) * (ux * R(p.force[2]) + uz * R(p.force[0])) : R(0);
         const R fyz = cm_force ? R(0.5) * (uy * R(p.force[2]) + uz * R(p.force[1])) : R(0);
         const R pxy = k110 - fxy, pxz = k101 - fxz, pyz = k011 - fyz;
-        const R s2 = pxx * pxx + pyy * pyy + pzz * pzz + R(2) * (pxy * pxy + pxz * pxz + pyz * pyz);
-        const R pi = sqrt(R(2) * s2) * irho;
-        const R tau0 = R(p.tau0);
-        om_sgs = R(2) / (tau0 + sqrt(R(p.sgs_c18) * pi + tau0 * tau0));
+        if constexpr (CLOSURE) {
+            om_sgs = R(1) / (R(p.tau0) + R(3) * nu_t(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz));
+        } else {
+            const R s2 = pxx * pxx + pyy * pyy + pzz * pzz + R(2) * (pxy * pxy + pxz * pxz + pyz * pyz);
+            const R pi = sqrt(R(2) * s2) * irho;
+            const R tau0 = R(p.tau0);
+            om_sgs = R(2) / (tau0 + sqrt(R(p.sgs_c18) * pi + tau0 * tau0));
+        }
     }
     auto rate = [&](int idx) -> R {
         R r = R(p.rates[idx]);
-        if (p.sgs == 1 && ((p.sgs_mask >> idx) & 1u)) r = om_sgs;
+        if ((CLOSURE || p.sgs == 1) && ((p.sgs_mask >> idx) & 1u)) r = om_sgs;
         return r;
     };
     const R w_xy = rate(4), w_xz = rate(5), w_yz = rate(6), w_d1 = rate(7), w_d2 = rate(8), w_b = rate(9);
@@ -536,7 +544,7 @@ __device__ __forceinline__ R collide_cum_ho1(R (&f)[27], const Physics& p) {
     chimera_backward(d, uz, 1, 9, 3);
 #pragma unroll
     for (int i = 0; i < 27; ++i) f[i] = d[cube<27>(i)];
-    return p.sgs == 1 ? om_sgs : R(p.rates[4]);
+    return (CLOSURE || p.sgs == 1) ? om_sgs : R(p.rates[4]);
 }
 
 // ------------------------------------------------------------------ equilibria (setter)

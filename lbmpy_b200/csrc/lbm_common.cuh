@@ -11,7 +11,7 @@ namespace lbm {
 
 enum StoreType : int { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3 };
 // SRT/TRT | raw-moment MRT | cumulant | cumulant with every order >= 3 relaxed by 1
-enum MethodKind : int { MK_POP = 0, MK_MRT = 1, MK_CUM = 2, MK_CUM1 = 3 };
+enum MethodKind : int { MK_POP = 0, MK_MRT = 1, MK_CUM = 2, MK_CUM1 = 3, MK_CUM1_MLP = 4 };
 enum PatternKind : int { PAT_PULL = 0, PAT_AA_EVEN = 1, PAT_AA_ODD = 2, PAT_ESO_EVEN = 3, PAT_ESO_ODD = 4 };
 enum ForceKind : int { FM_NONE = 0, FM_GUO = 1, FM_CENTRAL = 2, FM_SIMPLE = 3, FM_LUO = 4 };
 

@@ -168,4 +168,11 @@ LBM_DECLARE_FAMILY(q27_mrt)
 LBM_DECLARE_FAMILY(q27_cum)
 LBM_DECLARE_FAMILY(q27_cum1)
 
+// error reporting shared by the entry points of every translation unit (lbm_abi.cu)
+int abi_fail(int code, const char* fmt, ...);
+
+// learned closure (lbm_q27_closure.cu)
+SweepLauncher sweep_q27_closure(int store, int pat);
+cudaError_t closure_upload(const float* host_params, cudaStream_t stream);
+
 }  // namespace lbm

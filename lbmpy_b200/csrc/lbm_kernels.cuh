@@ -52,11 +52,17 @@ template <int PAT> struct PrevPattern {
                                : PAT_PULL;
 };
 
+// Eddy viscosity of the learned closure for the sweep with MK_CUM1_MLP; defined (with the
+// constant-memory parameters it reads) only in the translation unit that instantiates that
+// sweep, lbm_q27_closure.cu.
+template <class R> struct ClosureNu;
+
 template <class R, int Q, int MK>
 __device__ __forceinline__ R collide(R (&f)[Q], const Physics& p) {
     if constexpr (MK == MK_POP) return collide_pop<Q, R>(f, p);
     else if constexpr (MK == MK_MRT) return collide_mrt<Q, R>(f, p);
     else if constexpr (MK == MK_CUM1) return collide_cum_ho1<R>(f, p);
+    else if constexpr (MK == MK_CUM1_MLP) return collide_cum_ho1<R, true>(f, p, ClosureNu<R>{});
     else return collide_cum<R>(f, p);
 }
 
@@ -117,11 +123,14 @@ template <class S, class R, int Q, int MK, int PAT>
 __device__ __forceinline__ void sweep_cell(const SweepArgs& a, int x, int y, int z) {
     using A = Access<PAT>;
     const Grid& g = a.g;
-    int fl = 0;
-    if (g.flags != nullptr) {
-        fl = g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz];
-        if (fl & FLAG_TYPE_MASK) return;
-    }
+    // Flag first or together with the populations.  Every address below lies inside the
+    // ghost-inclusive field whatever the cell type, so the populations can be loaded before the
+    // flag is known: a boundary cell wastes a few loads, and no cell waits for a flag round trip
+    // before its loads issue.  The specialised cumulant sweep keeps the flag first: its register
+    // budget (64 per thread for AA) does not hold the flag alongside 27 loads in flight.
+    constexpr bool flag_first = MK == MK_CUM1 || MK == MK_CUM1_MLP;
+    const int fl = g.flags != nullptr ? g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz] : 0;
+    if (flag_first && (fl & FLAG_TYPE_MASK)) return;
     NbrOffsets nb;
     nb.init(g, x, y, z);
     const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
@@ -133,6 +142,7 @@ __device__ __forceinline__ void sweep_cell(const SweepArgs& a, int x, int y, int
         const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
         f[i] = Conv<S, R>::ld(src + eidx(A::template rslot<Q>(i) * g.sq, cell + off));
     }
+    if (!flag_first && (fl & FLAG_TYPE_MASK)) return;
     if (fl & FLAG_NEAR_WALL) bounce_back<S, R, Q, PAT>(f, a, nb, cell, x, y, z);
     const R om = collide<R, Q, MK>(f, a.p);
 #pragma unroll
@@ -172,13 +182,14 @@ struct BatchArgs {
 };
 
 template <class S, class R, int Q, int MK, int PAT>
-__global__ void __launch_bounds__(256) k_sweep_batched(const BatchArgs b) {
+__global__ void __launch_bounds__(256, 2) k_sweep_batched(const BatchArgs b) {
     __shared__ __align__(16) SweepArgs sa;
     constexpr int WORDS = sizeof(SweepArgs) / 4;
     static_assert(sizeof(SweepArgs) % 4 == 0, "SweepArgs is copied as 32-bit words");
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
     const int nthreads = blockDim.x * blockDim.y;
     int staged = -1;
+#pragma unroll 1
     for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
         const BatchTile tile = b.tiles[t];
         if (tile.domain != staged) {
@@ -193,6 +204,7 @@ __global__ void __launch_bounds__(256) k_sweep_batched(const BatchArgs b) {
         const int y = tile.y0 + threadIdx.y;
         if (x < sa.g.nx && y < sa.g.ny) {
             const int z1 = min(tile.z0 + b.cells_z, sa.g.nz);
+#pragma unroll 1
             for (int z = tile.z0; z < z1; ++z) sweep_cell<S, R, Q, MK, PAT>(sa, x, y, z);
         }
     }

@@ -60,6 +60,7 @@ class ForceModel(Enum):
 class SubgridScaleModel(Enum):
     SMAGORINSKY = auto()
     QR = auto()
+    LEARNED = auto()        # learned eddy viscosity (closure.MLPClosure); not an lbmpy model
 
 
 class Target(Enum):

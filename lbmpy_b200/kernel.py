@@ -91,8 +91,10 @@ def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None,
     shear = _evaluate(m.shear_relaxation_rate, params, ph)
     d.shear_rate = shear
     if rule.subgrid_scale_model is not None:
-        d.sgs = N.SGS_SMAGORINSKY
-        d.sgs_constant = float(rule.smagorinsky_constant)
+        from .enums import SubgridScaleModel
+        learned = rule.subgrid_scale_model == SubgridScaleModel.LEARNED
+        d.sgs = N.SGS_MLP if learned else N.SGS_SMAGORINSKY
+        d.sgs_constant = 0.0 if learned else float(rule.smagorinsky_constant)
         mask = 0
         # every moment whose (numeric) rate equals the shear rate is adapted, as lbmpy substitutes the
         # shared rate symbol (methods/abstractlbmethod.py:102-131, turbulence_models.py:55-63)
@@ -158,6 +160,9 @@ class LbKernel:
 
     def plan(self, dims, periodic, params=None, ubb_velocities=None) -> N.Plan:
         desc = build_desc(self.update_rule, dims, periodic, params or {}, ubb_velocities)
+        closure = self.update_rule.collision_rule.closure
+        if closure is not None:
+            closure.ensure_uploaded()
         key = (tuple(dims), tuple(bool(p) for p in periodic), torch.cuda.current_device())
         p = self._plans.get(key)
         if p is None:

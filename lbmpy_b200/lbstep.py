@@ -198,6 +198,9 @@ class LatticeBoltzmannStep:
             self._bound_sweep = k.bind(self.pdfs, self.periodicity, flags, bh.ubb_velocities, self.kernel_params)
             self._bound_key = (id(bh._dev), bh._dev is None, tuple(sorted(self.kernel_params.items())),
                                torch.cuda.current_stream().cuda_stream)
+        closure = self._kernels[0].update_rule.collision_rule.closure
+        if closure is not None:
+            closure.ensure_uploaded()          # a retrained closure reaches the next sweep
         return self._bound_sweep
 
     def set_pdf_fields_from_macroscopic_values(self):

@@ -31,6 +31,9 @@
 
 #define QMAX 27
 #define TMAX 40
+#define MLP_NIN 10
+#define MLP_NH 32
+#define MLP_NPARAM (MLP_NIN * MLP_NH + MLP_NH + MLP_NH * MLP_NH + MLP_NH + MLP_NH + 1 + 1)
 
 typedef struct {
     int D, Q;
@@ -48,9 +51,10 @@ typedef struct {
     int force_model;          /* 0 none, 1 Guo, 2 CentralMoment, 3 Simple, 4 Luo */
     double F[3];
     int galilean;
-    int sgs;                  /* 0 none, 1 Smagorinsky */
+    int sgs;                  /* 0 none, 1 Smagorinsky, 2 learned eddy viscosity (MLP) */
     double sgs_c;
     double shear_rate;
+    float mlp[MLP_NPARAM];    /* sgs == 2: W1[10][32] b1[32] W2[32][32] b2[32] W3[32] b3 scale */
 } om_method;
 
 typedef struct {
@@ -322,6 +326,66 @@ static void populations_from_central(const om_method* m, const double* km, const
     (void)c; (void)v;
 }
 
+/* Learned eddy viscosity: features of the pre-collision non-equilibrium stress P (3x3), density
+ * and velocity, then a 10-32-32-1 perceptron (SiLU hidden units, softplus output times a fixed
+ * scale), evaluated in FP64 with the FP32 parameters.  nu_t enters as omega = 1/(tau0 + 3 nu_t),
+ * on the moments whose rate is the shear rate, as the Smagorinsky model does
+ * (turbulence_models.py:25-84). */
+static void mlp_features(const double P[3][3], double rho, const double u[3], double x[MLP_NIN]) {
+    double s2 = 0.0, off2, tr, d[3][3], d2 = 0.0, dn, tr3 = 0.0, u2, uau = 0.0, mx = 0.0, pim;
+    int a, b, c;
+    for (a = 0; a < 3; ++a) for (b = 0; b < 3; ++b) s2 += P[a][b] * P[a][b];
+    off2 = P[0][1] * P[0][1] + P[0][2] * P[0][2] + P[1][2] * P[1][2];
+    tr = P[0][0] + P[1][1] + P[2][2];
+    for (a = 0; a < 3; ++a) for (b = 0; b < 3; ++b) d[a][b] = P[a][b] - (a == b ? tr / 3.0 : 0.0);
+    for (a = 0; a < 3; ++a) for (b = 0; b < 3; ++b) d2 += d[a][b] * d[a][b];
+    dn = sqrt(d2);
+    for (a = 0; a < 3; ++a) for (b = 0; b < 3; ++b) for (c = 0; c < 3; ++c) tr3 += d[a][b] * d[b][c] * d[c][a];
+    u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    for (a = 0; a < 3; ++a) for (b = 0; b < 3; ++b) uau += u[a] * d[a][b] * u[b];
+    for (a = 0; a < 3; ++a) if (fabs(d[a][a]) > mx) mx = fabs(d[a][a]);
+    pim = sqrt(2.0 * s2) / rho;
+    x[0] = log(pim + 1e-9);
+    x[1] = 100.0 * pim;
+    x[2] = tr / (sqrt(s2) + 1e-12);
+    x[3] = sqrt(6.0) * tr3 / (d2 * dn + 1e-30);
+    x[4] = 30.0 * sqrt(u2);
+    x[5] = 1000.0 * (rho - 1.0);
+    x[6] = uau / ((u2 + 1e-12) * dn + 1e-30);
+    x[7] = off2 / (s2 + 1e-30);
+    x[8] = mx / (dn + 1e-30);
+    x[9] = 1000.0 * u2;
+}
+
+static double silu(double z) { return z / (1.0 + exp(-z)); }
+
+double om_mlp_nu_t(const float* w, const double x[MLP_NIN]) {
+    const float* W1 = w;
+    const float* b1 = W1 + MLP_NIN * MLP_NH;
+    const float* W2 = b1 + MLP_NH;
+    const float* b2 = W2 + MLP_NH * MLP_NH;
+    const float* W3 = b2 + MLP_NH;
+    const float* b3 = W3 + MLP_NH;
+    double h1[MLP_NH], y = b3[0];
+    int i, j, k;
+    for (k = 0; k < MLP_NH; ++k) {
+        double z = b1[k];
+        for (i = 0; i < MLP_NIN; ++i) z += x[i] * W1[i * MLP_NH + k];
+        h1[k] = silu(z);
+    }
+    for (k = 0; k < MLP_NH; ++k) {
+        double z = b2[k];
+        for (j = 0; j < MLP_NH; ++j) z += h1[j] * W2[j * MLP_NH + k];
+        y += silu(z) * W3[k];
+    }
+    return (double)b3[1] * (y > 20.0 ? y : log1p(exp(y)));
+}
+
+void om_mlp_features(const double* P6, double rho, const double* u, double* x) {
+    double P[3][3] = {{P6[0], P6[3], P6[4]}, {P6[3], P6[1], P6[5]}, {P6[4], P6[5], P6[2]}};
+    mlp_features(P, rho, u, x);
+}
+
 static void collide_cumulant(const om_method* m, const double* f, double* fo, double* omega_out,
                              int all_rates_one) {
     int Q = m->Q, i, k, d, n;
@@ -351,7 +415,7 @@ static void collide_cumulant(const om_method* m, const double* f, double* fo, do
         cpoly[k] = s;
         rates[k] = all_rates_one ? 1.0 : m->rate[k];
     }
-    if (m->sgs == 1 && !all_rates_one) {
+    if ((m->sgs == 1 || m->sgs == 2) && !all_rates_one) {
         /* f_neq = f - f_eq with f_eq = the rates-one collision (cumulantbasedmethod.py:220-240) */
         double feq[27], pi[3][3] = {{0}}, pn = 0.0, tau0, om; int a, b;
         collide_cumulant(m, f, feq, 0, 1);
@@ -361,7 +425,13 @@ static void collide_cumulant(const om_method* m, const double* f, double* fo, do
         for (a = 0; a < 3; ++a) for (b = 0; b < 3; ++b) pn += pi[a][b] * pi[a][b];
         pn = sqrt(2.0 * pn) / rho;
         tau0 = 1.0 / m->shear_rate;
-        om = 2.0 / (tau0 + sqrt(18.0 * m->sgs_c * m->sgs_c * pn + tau0 * tau0));
+        if (m->sgs == 1) {
+            om = 2.0 / (tau0 + sqrt(18.0 * m->sgs_c * m->sgs_c * pn + tau0 * tau0));
+        } else {
+            double x[MLP_NIN];
+            mlp_features(pi, rho, u, x);
+            om = 1.0 / (tau0 + 3.0 * om_mlp_nu_t(m->mlp, x));
+        }
         for (k = 0; k < Q; ++k) if (m->rate[k] == m->shear_rate) rates[k] = om;
         if (omega_out) *omega_out = om;
     }

@@ -21,6 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
 QMAX, TMAX = 27, 40
+MLP_NPARAM = 10 * 32 + 32 + 32 * 32 + 32 + 32 + 1 + 1
 PATTERNS = {"pull": 0, "push": 1, "aa": 2, "esotwist": 3}
 
 
@@ -45,6 +46,7 @@ class OmMethod(ctypes.Structure):
         ("sgs", ctypes.c_int),
         ("sgs_c", ctypes.c_double),
         ("shear_rate", ctypes.c_double),
+        ("mlp", ctypes.c_float * MLP_NPARAM),
     ]
 
 
@@ -137,6 +139,10 @@ class Oracle:
         m.sgs = method.sgs
         m.sgs_c = method.sgs_constant
         m.shear_rate = method.shear_rate
+        if method.mlp is not None:
+            w = np.asarray(method.mlp, dtype=np.float32).reshape(-1)
+            assert w.size == MLP_NPARAM, f"closure parameters: {w.size} != {MLP_NPARAM}"
+            ctypes.memmove(ctypes.addressof(m.mlp), w.ctypes.data, w.nbytes)
         self._m = m
         self.M = np.array([[float(v) for v in r] for r in M])
         self.Minv = np.array([[float(v) for v in r] for r in Minv])
@@ -257,3 +263,23 @@ class Oracle:
 
 def make(stencil, method, **kw) -> Oracle:
     return Oracle(spec.resolve(stencil, method, **kw))
+
+
+def mlp_features(P6, rho, u):
+    """Closure features of one cell from the C restatement (om_mlp_features)."""
+    P6 = np.ascontiguousarray(P6, np.float64)
+    uu = np.ascontiguousarray(u, np.float64)
+    x = np.zeros(10)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib().om_mlp_features(P6.ctypes.data_as(dp), ctypes.c_double(float(rho)), uu.ctypes.data_as(dp),
+                          x.ctypes.data_as(dp))
+    return x
+
+
+def mlp_nu_t(params, x):
+    """nu_t of one feature vector from the C restatement (om_mlp_nu_t)."""
+    w = np.ascontiguousarray(params, np.float32)
+    xx = np.ascontiguousarray(x, np.float64)
+    f = lib().om_mlp_nu_t
+    f.restype = ctypes.c_double
+    return f(w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), xx.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))

@@ -313,7 +313,7 @@ def magic_rate(omega, magic=Fraction(3, 16)):
 # --------------------------------------------------------------------------------------------
 KIND_MOMENT, KIND_CUMULANT = 0, 1
 FORCE_NONE, FORCE_GUO, FORCE_CENTRAL_MOMENT, FORCE_SIMPLE, FORCE_LUO = 0, 1, 2, 3, 4
-SGS_NONE, SGS_SMAGORINSKY = 0, 1
+SGS_NONE, SGS_SMAGORINSKY, SGS_MLP = 0, 1, 2
 
 
 @dataclass
@@ -334,6 +334,7 @@ class OracleMethod:
     sgs: int = SGS_NONE
     sgs_constant: float = 0.12
     shear_rate: float = 0.0
+    mlp: object = None            # learned-closure parameters (float32 array) when sgs == SGS_MLP
 
     @property
     def Q(self):
@@ -347,7 +348,7 @@ class OracleMethod:
 def resolve(stencil: str, method: str, relaxation_rate=None, relaxation_rates=None,
             compressible=False, zero_centered=True, delta_equilibrium=None,
             equilibrium_order=2, force=(0.0, 0.0, 0.0), force_model=None,
-            galilean_correction=False, smagorinsky=None) -> OracleMethod:
+            galilean_correction=False, smagorinsky=None, mlp=None) -> OracleMethod:
     """Follows ``LBMConfig.__post_init__`` (creationfunctions.py:347-484) and
     ``create_lb_method`` (creationfunctions.py:773-868) for SRT/TRT/MRT/CUMULANT."""
     method = method.lower()
@@ -406,9 +407,11 @@ def resolve(stencil: str, method: str, relaxation_rate=None, relaxation_rates=No
     if smagorinsky is not None:
         sgs = SGS_SMAGORINSKY
         c_sgs = 0.12 if smagorinsky is True else float(smagorinsky)
+    if mlp is not None:
+        sgs = SGS_MLP
     return OracleMethod(stencil=stencil, kind=kind, dirs=dirs, weights=w, moments=moments,
                         rates=[float(r) for r in rates], compressible=bool(compressible),
                         zero_centered=bool(zero_centered), delta_equilibrium=bool(delta_equilibrium),
                         equilibrium_order=equilibrium_order, force_model=fm, force=force,
                         galilean_correction=bool(galilean_correction), sgs=sgs, sgs_constant=c_sgs,
-                        shear_rate=float(shear))
+                        shear_rate=float(shear), mlp=mlp)

@@ -6,6 +6,7 @@
 #include <cmath>
 using std::sqrt;
 #include "../../lbmpy_b200/csrc/lbm_collide.cuh"
+#include "../../lbmpy_b200/csrc/lbm_closure.cuh"
 
 using namespace lbm;
 
@@ -35,6 +36,14 @@ static double runf(double* f, const Physics* p) {
     return om;
 }
 
+template <class R> struct HostClosureNu {
+    const float* w;
+    R operator()(R pxx, R pyy, R pzz, R pxy, R pxz, R pyz, R rho, R ux, R uy, R uz) const {
+        R x[MLP_IN];
+        closure_features<R>(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz, x);
+        return closure_nu_t<R>(x, w);
+    }
+};
 extern "C" {
 int host_sizeof_physics() { return (int)sizeof(Physics); }
 double host_collide(int q, int mk, int fp32, double* f, const Physics* p) {
@@ -45,6 +54,31 @@ double host_collide(int q, int mk, int fp32, double* f, const Physics* p) {
     if (q == 27 && mk == MK_CUM) return fp32 ? runf<27, MK_CUM>(f, p) : run<27, MK_CUM>(f, p);
     if (q == 27 && mk == MK_CUM1) return fp32 ? runf<27, MK_CUM1>(f, p) : run<27, MK_CUM1>(f, p);
     return -1.0;
+}
+// learned closure: features, network, and the cumulant collision with the closure folded in
+void host_closure_features(const double* s10, double* x) {
+    double xx[MLP_IN];
+    closure_features<double>(s10[0], s10[1], s10[2], s10[3], s10[4], s10[5], s10[6], s10[7], s10[8], s10[9], xx);
+    for (int i = 0; i < MLP_IN; ++i) x[i] = xx[i];
+}
+double host_closure_nu_t(const double* x, const float* w) {
+    double xx[MLP_IN];
+    for (int i = 0; i < MLP_IN; ++i) xx[i] = x[i];
+    return closure_nu_t<double>(xx, w);
+}
+double host_collide_closure(int fp32, double* f, const Physics* p, const float* w) {
+    if (fp32) {
+        float g[27];
+        for (int i = 0; i < 27; ++i) g[i] = (float)f[i];
+        const float om = collide_cum_ho1<float, true>(g, *p, HostClosureNu<float>{w});
+        for (int i = 0; i < 27; ++i) f[i] = g[i];
+        return om;
+    }
+    double g[27];
+    for (int i = 0; i < 27; ++i) g[i] = f[i];
+    const double om = collide_cum_ho1<double, true>(g, *p, HostClosureNu<double>{w});
+    for (int i = 0; i < 27; ++i) f[i] = g[i];
+    return om;
 }
 void host_equilibrium(int q, int mk, double* f, double rho, double ux, double uy, double uz, const Physics* p) {
     if (q == 19 && mk == MK_POP) { double g[19]; equilibrium<19, double, MK_POP>(g, rho, ux, uy, uz, *p); for (int i = 0; i < 19; ++i) f[i] = g[i]; }
