@@ -23,6 +23,8 @@ struct LbmPlan {
     int device;
     int q, mk, store;
     int use_pair;          // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_PAIR)
+    int zc;                // z-planes per thread of the FP32 closure sweep (environment LBM_B200_ZC, else 8)
+    void* ubb_rho;         // compressible + moving UBB walls: density gathered before the sweep
     Physics phys;
     double* partial;       // reduction scratch: RED_BLOCKS * 5 doubles
     double* red_out;       // 5 doubles on the device
@@ -108,7 +110,7 @@ Grid make_grid(const LbmPlan* p, const int64_t s[4], const uint8_t* flags) {
 
 // 256-thread blocks shaped along x: the widest of 128 / 64 / 32 threads whose last block in a
 // row idles at most 1/8 of the row (else 32).
-void launch_shape(const Grid& g, dim3& grid, dim3& block) {
+void launch_shape(const Grid& g, int zc, dim3& grid, dim3& block) {
     int bx = 32;
     for (int c : {128, 64}) {
         const int waste = (g.nx + c - 1) / c * c - g.nx;
@@ -116,7 +118,7 @@ void launch_shape(const Grid& g, dim3& grid, dim3& block) {
     }
     const int by = 256 / bx;
     block = dim3(bx, by, 1);
-    grid = dim3((g.nx + bx - 1) / bx, (g.ny + by - 1) / by, g.nz);
+    grid = dim3((g.nx + bx - 1) / bx, (g.ny + by - 1) / by, (g.nz + zc - 1) / zc);
 }
 
 int pattern_kind(const LbmPlan* p, int parity) {
@@ -243,6 +245,58 @@ ReduceLauncher reduce_launcher_q(int store, int pat) {
         case ST_BF16: return pick_reduce<__nv_bfloat16, Q>(pat);
     }
     return nullptr;
+}
+
+// ---- previous-step density next to moving walls (k_ubb_density)
+using UbbLauncher = cudaError_t (*)(const SweepArgs&, void*, dim3, dim3, cudaStream_t);
+
+template <class S, class R, int Q, int PAT>
+cudaError_t launch_ubb(const SweepArgs& a, void* out, dim3 grid, dim3 block, cudaStream_t s) {
+    k_ubb_density<S, R, Q, PAT><<<grid, block, 0, s>>>(a, static_cast<R*>(out));
+    return cudaGetLastError();
+}
+
+template <class S, class R, int Q>
+UbbLauncher pick_ubb(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_ubb<S, R, Q, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_ubb<S, R, Q, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_ubb<S, R, Q, PAT_AA_ODD>;
+        case PAT_ESO_EVEN: return &launch_ubb<S, R, Q, PAT_ESO_EVEN>;
+        case PAT_ESO_ODD: return &launch_ubb<S, R, Q, PAT_ESO_ODD>;
+    }
+    return nullptr;
+}
+
+template <int Q>
+UbbLauncher ubb_launcher_q(int store, int pat) {
+    switch (store) {
+        case ST_F64: return pick_ubb<double, double, Q>(pat);
+        case ST_F32: return pick_ubb<float, float, Q>(pat);
+        case ST_F16: return pick_ubb<__half, float, Q>(pat);
+        case ST_BF16: return pick_ubb<__nv_bfloat16, float, Q>(pat);
+    }
+    return nullptr;
+}
+
+// The compressible UBB of a moving wall needs the cell's previous-step density.
+bool needs_ubb_density(const LbmPlanDesc* d) {
+    if (!d->compressible) return false;
+    for (int u = 0; u < 4; ++u)
+        for (int k = 0; k < 3; ++k)
+            if (d->ubb_velocity[u][k] != 0.0) return true;
+    return false;
+}
+
+int ensure_ubb_buffer(LbmPlan* p) {
+    if (!needs_ubb_density(&p->desc) || p->ubb_rho != nullptr) return LBM_OK;
+    const size_t n = size_t(p->desc.dims[0]) * p->desc.dims[1] * p->desc.dims[2];
+    cudaError_t e = cudaMalloc(&p->ubb_rho, n * (p->store == ST_F64 ? 8 : 4));
+    if (e != cudaSuccess) {
+        p->ubb_rho = nullptr;
+        return cuda_fail(e, "cudaMalloc(wall density)");
+    }
+    return LBM_OK;
 }
 
 // Marks fluid cells that have a boundary neighbour along the stencil.
@@ -380,6 +434,9 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
     {
         const char* env = getenv("LBM_B200_PAIR");
         p->use_pair = env == nullptr ? -1 : (env[0] == '0' ? 0 : 1);
+        const char* zenv = getenv("LBM_B200_ZC");
+        p->zc = zenv != nullptr ? atoi(zenv) : 8;
+        if (p->zc < 1) p->zc = 1;
     }
     fill_physics(p, desc);
     int sms = 148;
@@ -388,10 +445,16 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
     e = cudaMalloc(&p->partial, sizeof(double) * 5 * (p->red_blocks + 1));
     if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaMalloc(reduction scratch)"); }
     p->red_out = p->partial + 5 * p->red_blocks;
+    p->ubb_rho = nullptr;
     if (sweep_launcher(p, PAT_PULL) == nullptr) {
         cudaFree(p->partial);
         delete p;
         return fail(LBM_E_UNSUPPORTED, "no kernel built for this stencil/method/dtype");
+    }
+    if (int rc2 = ensure_ubb_buffer(p)) {
+        cudaFree(p->partial);
+        delete p;
+        return rc2;
     }
     *out = p;
     return LBM_OK;
@@ -408,12 +471,13 @@ int lbm_plan_update(LbmPlan* p, const LbmPlanDesc* desc) {
     p->desc = *desc;
     p->mk = method_kind(desc);
     fill_physics(p, desc);
-    return LBM_OK;
+    return ensure_ubb_buffer(p);
 }
 
 int lbm_plan_destroy(LbmPlan* p) {
     if (p == nullptr) return LBM_OK;
     if (p->partial) cudaFree(p->partial);
+    if (p->ubb_rho) cudaFree(p->ubb_rho);
     delete p;
     return LBM_OK;
 }
@@ -444,6 +508,18 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
     a.src = src;
     a.dst = dst;
     a.omega_out = omega_out;
+    a.zc = (p->mk == MK_CUM1_MLP && p->store == ST_F32) ? p->zc : 1;
+    a.pad_ = 0;
+    a.ubb_rho = nullptr;
+    if (flags != nullptr && p->ubb_rho != nullptr && needs_ubb_density(&p->desc)) {
+        UbbLauncher U = p->q == 19 ? ubb_launcher_q<19>(p->store, pat) : ubb_launcher_q<27>(p->store, pat);
+        if (U == nullptr) return fail(LBM_E_UNSUPPORTED, "no wall-density kernel for this storage type / pattern");
+        dim3 ug, ub;
+        launch_shape(a.g, 1, ug, ub);
+        cudaError_t e = U(a, p->ubb_rho, ug, ub, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "wall-density launch");
+        a.ubb_rho = p->ubb_rho;
+    }
     dim3 grid, block;
     SweepLauncher L;
     if (pair_applicable(p, src, dst, strides, pat, omega_out)) {
@@ -452,7 +528,7 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
         grid = dim3((a.g.nx + 63) / 64, (a.g.ny + PAIR_ROWS - 1) / PAIR_ROWS, a.g.nz);
     } else {
         L = sweep_launcher(p, pat);
-        launch_shape(a.g, grid, block);
+        launch_shape(a.g, a.zc, grid, block);
     }
     if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no kernel for this storage type / pattern");
     cudaError_t e = L(a, grid, block, stream);
@@ -521,7 +597,7 @@ int lbm_set_equilibrium(const LbmPlan* p, void* pdfs, const int64_t strides[4], 
     MacroLauncher L = set_eq_launcher(p, pattern_kind(p, prev_parity ? 1 : 0));
     if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no setter kernel");
     dim3 grid, block;
-    launch_shape(a.g, grid, block);
+    launch_shape(a.g, 1, grid, block);
     cudaError_t e = L(a, grid, block, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? LBM_OK : cuda_fail(e, "setter launch");
 }
@@ -537,7 +613,7 @@ int lbm_get_macroscopic(const LbmPlan* p, const void* pdfs, const int64_t stride
     MacroLauncher L = p->q == 19 ? get_launcher_q<19>(p->store, pat) : get_launcher_q<27>(p->store, pat);
     if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no getter kernel");
     dim3 grid, block;
-    launch_shape(a.g, grid, block);
+    launch_shape(a.g, 1, grid, block);
     cudaError_t e = L(a, grid, block, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? LBM_OK : cuda_fail(e, "getter launch");
 }
@@ -584,7 +660,7 @@ int lbm_flags_finalize(const LbmPlan* p, uint8_t* flags, void* stream) {
     int64_t s[4] = {1, p->desc.dims[0] + 2, (int64_t)(p->desc.dims[0] + 2) * (p->desc.dims[1] + 2), 0};
     Grid g = make_grid(p, s, flags);
     dim3 grid, block;
-    launch_shape(g, grid, block);
+    launch_shape(g, 1, grid, block);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (p->q == 19) k_flags_finalize<19><<<grid, block, 0, st>>>(g);
     else k_flags_finalize<27><<<grid, block, 0, st>>>(g);
@@ -707,6 +783,9 @@ int lbm_batch_create(const LbmPlanDesc* common, const LbmDomainDesc* domains, in
             return fail(LBM_E_INVALID, "domain %d: flags_offset must be >= 0 or -1", k);
         }
         if (!cumulant_high_orders_relax_to_equilibrium(&pk.desc)) all_cum1 = false;
+        if (needs_ubb_density(&pk.desc) && d.flags_offset >= 0)
+            return fail(LBM_E_UNSUPPORTED, "domain %d: moving UBB walls of a compressible method are not built "
+                        "for batches", k);
         cells += int64_t(d.dims[0]) * d.dims[1] * d.dims[2];
     }
     if (!disjoint(fields)) return fail(LBM_E_INVALID, "two domains' fields overlap");

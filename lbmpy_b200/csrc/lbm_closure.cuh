@@ -18,6 +18,7 @@
 #endif
 
 #include <cmath>
+#include <cstdint>
 #include <type_traits>
 
 namespace lbm {
@@ -159,5 +160,133 @@ template <class R, class WA, bool FULL = true, bool SWEEP = false>
 LBM_HD R closure_nu_t(const R (&x)[MLP_IN], const WA& w) {
     return R(w[MLP_SCALE]) * mlp_softplus<R>(mlp_output<R, WA, FULL, SWEEP>(x, w));
 }
+
+#ifdef __CUDACC__
+// ------------------------------------------------------------------ tensor-core inference (FP32)
+// The network for the 32 cells of a warp at once: each layer is a 32 x K by K x 32 product done
+// as m16n8k8 TF32 tiles (mma.sync; rows are the warp's cells), the hidden activations pass
+// through a per-warp shared-memory tile of 32 rows.  TF32 operands (10-bit mantissa) give nu_t to
+// about 1e-3 relative; training and the FP64 sweep use the exact network.
+
+constexpr int MLP_TLD = 33;                       // row stride of the per-warp activation tile
+
+__device__ __forceinline__ uint32_t to_tf32(float v) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+    return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Parameter block as the tensor-core network reads it from shared memory: the entries of W1 and
+// W2 as TF32 bit patterns, everything else as FP32 bit patterns.
+template <class WA>
+__device__ __forceinline__ void stage_mlp_params(const WA& w, uint32_t* sw, int tid, int nthreads) {
+    for (int i = tid; i < MLP_PARAMS; i += nthreads) {
+        const float v = w[i];
+        const bool matrix = i < MLP_B1 || (i >= MLP_W2 && i < MLP_B2);
+        sw[i] = matrix ? to_tf32(v) : __float_as_uint(v);
+    }
+}
+
+// nu_t of this lane's cell; every lane of the warp must call it together.  T: this warp's
+// 32 x MLP_TLD float tile.
+__device__ __forceinline__ float warp_mlp_nu(const float (&x)[MLP_IN], const uint32_t* sw, float* T) {
+    const int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
+    const int gid = lane >> 2, t4 = lane & 3;
+    auto F = [&](int i) { return __uint_as_float(sw[i]); };
+#pragma unroll
+    for (int k = 0; k < 16; ++k) T[lane * MLP_TLD + k] = k < MLP_IN ? x[k] : 0.f;
+    __syncwarp();
+    float acc[2][4][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[mt][nt][c] = 0.f;
+    // layer 1: [32 x 16] (features, zero-padded) x [16 x 32]
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            const int r0 = (mt * 16 + gid) * MLP_TLD, r1 = r0 + 8 * MLP_TLD, c0 = ks * 8 + t4;
+            const uint32_t a0 = to_tf32(T[r0 + c0]), a1 = to_tf32(T[r1 + c0]);
+            const uint32_t a2 = to_tf32(T[r0 + c0 + 4]), a3 = to_tf32(T[r1 + c0 + 4]);
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int n = nt * 8 + gid;
+                const uint32_t b0 = c0 < MLP_IN ? sw[MLP_W1 + c0 * MLP_H + n] : 0u;
+                const uint32_t b1 = c0 + 4 < MLP_IN ? sw[MLP_W1 + (c0 + 4) * MLP_H + n] : 0u;
+                mma_tf32(acc[mt][nt], a0, a1, a2, a3, b0, b1);
+            }
+        }
+    __syncwarp();
+    // bias + SiLU, back into the tile as rows of 32 hidden units
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int col = nt * 8 + 2 * t4, r0 = (mt * 16 + gid) * MLP_TLD, r1 = r0 + 8 * MLP_TLD;
+            const float blo = F(MLP_B1 + col), bhi = F(MLP_B1 + col + 1);
+            T[r0 + col] = mlp_silu_sweep<float>(acc[mt][nt][0] + blo);
+            T[r0 + col + 1] = mlp_silu_sweep<float>(acc[mt][nt][1] + bhi);
+            T[r1 + col] = mlp_silu_sweep<float>(acc[mt][nt][2] + blo);
+            T[r1 + col + 1] = mlp_silu_sweep<float>(acc[mt][nt][3] + bhi);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[mt][nt][c] = 0.f;
+        }
+    __syncwarp();
+    // layer 2: [32 x 32] x [32 x 32]
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+            const int r0 = (mt * 16 + gid) * MLP_TLD, r1 = r0 + 8 * MLP_TLD, c0 = ks * 8 + t4;
+            const uint32_t a0 = to_tf32(T[r0 + c0]), a1 = to_tf32(T[r1 + c0]);
+            const uint32_t a2 = to_tf32(T[r0 + c0 + 4]), a3 = to_tf32(T[r1 + c0 + 4]);
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int n = nt * 8 + gid;
+                mma_tf32(acc[mt][nt], a0, a1, a2, a3, sw[MLP_W2 + c0 * MLP_H + n], sw[MLP_W2 + (c0 + 4) * MLP_H + n]);
+            }
+        }
+    // output unit: per-lane partial sums over its columns, then over the 4 lanes of a row group
+    float y[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int col = nt * 8 + 2 * t4;
+            const float blo = F(MLP_B2 + col), bhi = F(MLP_B2 + col + 1);
+            const float wlo = F(MLP_W3 + col), whi = F(MLP_W3 + col + 1);
+            y[mt][0] += mlp_silu_sweep<float>(acc[mt][nt][0] + blo) * wlo +
+                        mlp_silu_sweep<float>(acc[mt][nt][1] + bhi) * whi;
+            y[mt][1] += mlp_silu_sweep<float>(acc[mt][nt][2] + blo) * wlo +
+                        mlp_silu_sweep<float>(acc[mt][nt][3] + bhi) * whi;
+        }
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            y[mt][h] += __shfl_xor_sync(0xffffffffu, y[mt][h], 1);
+            y[mt][h] += __shfl_xor_sync(0xffffffffu, y[mt][h], 2);
+        }
+    // row `lane` sits in tile lane >> 4, half (lane >> 3) & 1, row group lane & 7
+    const int src = 4 * (lane & 7);
+    const float v00 = __shfl_sync(0xffffffffu, y[0][0], src), v01 = __shfl_sync(0xffffffffu, y[0][1], src);
+    const float v10 = __shfl_sync(0xffffffffu, y[1][0], src), v11 = __shfl_sync(0xffffffffu, y[1][1], src);
+    const int mt = lane >> 4, half = (lane >> 3) & 1;
+    const float yv = (mt ? (half ? v11 : v10) : (half ? v01 : v00)) + F(MLP_B3);
+    __syncwarp();
+    return F(MLP_SCALE) * mlp_softplus<float>(yv);
+}
+#endif
 
 }  // namespace lbm

@@ -114,6 +114,9 @@ struct SweepArgs {
     const void* src;
     void* dst;
     float* omega_out;      // optional per-cell effective shear rate (interior, x fastest)
+    int zc;                // closure sweep: consecutive z-planes per thread (next plane prefetched to L2)
+    int pad_;
+    const void* ubb_rho;   // compressible moving walls: previous-step density of the cells next to them
 };
 
 // Neighbour offsets in elements for c in {-1, 0, +1} along each axis, with periodic wrap.

@@ -85,7 +85,6 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
         fo.init(gf, x, y, z);
     }
     const int fcell = (x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz;
-    R rho_w = R(-1);   // lazily computed wall density (UBB, compressible)
 #pragma unroll
     for (int i = 1; i < Q; ++i) {
         const int bt = g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK;
@@ -96,20 +95,12 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
         R v = Conv<S, R>::ld(src + eidx(PA::template wslot<Q>(j) * g.sq, cell + off));
         if (bt >= FLAG_UBB0) {
             const double* uw = a.p.ubb[bt - FLAG_UBB0];
-            R rho = R(1);
-            if (a.p.compressible) {
-                if (rho_w < R(0)) {
-                    R s = 0;
-#pragma unroll
-                    for (int k = 0; k < Q; ++k) {
-                        const int ok = nb.off(PA::template woff<Q>(k, 0), PA::template woff<Q>(k, 1),
-                                              PA::template woff<Q>(k, 2));
-                        s += Conv<S, R>::ld(src + eidx(PA::template wslot<Q>(k) * g.sq, cell + ok));
-                    }
-                    rho_w = R(1) + s;
-                }
-                rho = rho_w;
-            }
+            // compressible: the cell's density at the previous step, gathered before the sweep
+            // (k_ubb_density; in-place sweeps overwrite the values it is summed from).  Interior
+            // cell indices fit 32 bits (the host bounds the field below 2^32 elements).
+            const R rho = (a.p.compressible && a.ubb_rho != nullptr)
+                              ? static_cast<const R*>(a.ubb_rho)[x + g.nx * (y + g.ny * z)]
+                              : R(1);
             const R cu = R(L::cx(i)) * R(uw[0]) + R(L::cy(i)) * R(uw[1]) + R(L::cz(i)) * R(uw[2]);
             v += R(6) * R(L::w(i)) * cu * rho;
         }
@@ -160,6 +151,66 @@ __global__ void __launch_bounds__(256) k_sweep(const SweepArgs a) {
     const int z = blockIdx.z;
     if (x >= a.g.nx || y >= a.g.ny) return;
     sweep_cell<S, R, Q, MK, PAT>(a, x, y, z);
+}
+
+// Asks L2 for the lines one cell will pull (prefetch.global.L2 is a hint: no data returns, no
+// registers are held, and every address is one the sweep itself reads).
+template <class S, int Q, int PAT>
+__device__ __forceinline__ void prefetch_cell(const SweepArgs& a, int x, int y, int z) {
+    using A = Access<PAT>;
+    const Grid& g = a.g;
+    NbrOffsets nb;
+    nb.init(g, x, y, z);
+    const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
+    const S* src = static_cast<const S*>(a.src);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
+        const S* q = src + eidx(A::template rslot<Q>(i) * g.sq, cell + off);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(q));
+    }
+}
+
+// Density, at the previous step, of every fluid cell with a moving-wall (UBB) link, for the
+// compressible UBB: lbmpy takes it from the cell's own post-collision values in a boundary pass
+// before the sweep (boundaries/boundaryconditions.py:794-841).  Inside an in-place sweep the
+// neighbours overwrite those locations, and summing them inside any sweep costs every cell
+// registers, so they are summed here first, for every pattern.
+template <class S, class R, int Q, int PAT>
+__global__ void __launch_bounds__(256) k_ubb_density(const SweepArgs a, R* rho_out) {
+    using L = Lat<Q>;
+    using PA = Access<PrevPattern<PAT>::value>;
+    const Grid& g = a.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.nx || y >= g.ny) return;
+    const int fcell = (x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz;
+    const int fl = g.flags[fcell];
+    if ((fl & FLAG_TYPE_MASK) || !(fl & FLAG_NEAR_WALL)) return;
+    NbrOffsets fo;
+    {
+        Grid gf = g;
+        gf.sy = g.fsy;
+        gf.sz = g.fsz;
+        fo.init(gf, x, y, z);
+    }
+    bool moving = false;
+#pragma unroll
+    for (int i = 1; i < Q; ++i)
+        if ((g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK) >= FLAG_UBB0) moving = true;
+    if (!moving) return;
+    NbrOffsets nb;
+    nb.init(g, x, y, z);
+    const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
+    const S* src = static_cast<const S*>(a.src);
+    R s = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const int ok = nb.off(PA::template woff<Q>(k, 0), PA::template woff<Q>(k, 1), PA::template woff<Q>(k, 2));
+        s += Conv<S, R>::ld(src + eidx(PA::template wslot<Q>(k) * g.sq, cell + ok));
+    }
+    rho_out[x + g.nx * (y + g.ny * z)] = R(1) + s;
 }
 
 // ------------------------------------------------------------------ batched domains
