@@ -24,6 +24,7 @@ struct LbmPlan {
     int q, mk, store;
     int use_pair;          // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_PAIR)
     int zc;                // z-planes per thread of the FP32 closure sweep (environment LBM_B200_ZC, else 8)
+    int use_quad;          // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_QUAD)
     void* ubb_rho;         // compressible + moving UBB walls: density gathered before the sweep
     Physics phys;
     double* partial;       // reduction scratch: RED_BLOCKS * 5 doubles
@@ -152,6 +153,33 @@ SweepLauncher pair_launcher(const LbmPlan* p, int pat) {
 }
 
 size_t store_size(int store) { return store == ST_F64 ? 8 : (store == ST_F32 ? 4 : 2); }
+
+SweepLauncher quad_launcher(const LbmPlan* p, int pat) {
+    if (p->q == 19 && p->mk == MK_POP) return sweep_quad_q19_pop(p->store, pat);
+    if (p->q == 19 && p->mk == MK_MRT) return sweep_quad_q19_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_POP) return sweep_quad_q27_pop(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM) return sweep_quad_q27_cum(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM1) return sweep_quad_q27_cum1(p->store, pat);
+    return nullptr;
+}
+
+// The quad sweep (16-bit storage): four x-adjacent cells per thread, 8-byte accesses.  Needs
+// nx a multiple of 4 and interior cell x = 0 of every row and slot on an 8-byte boundary.
+// Default policy, from B200 measurements: SRT/TRT (D3Q19 TRT FP16 pull 61.3 -> 68.2 GLUPS at
+// 256^3, 62.8 -> 70.0 at 512^3); not the moment-space methods, whose larger collision state
+// spills (MRT) or loses occupancy (cumulant AA: 29.0 -> 25.9).
+bool quad_applicable(const LbmPlan* p, const void* src, const void* dst, const int64_t s[4], int pat,
+                     const float* omega_out) {
+    if (p->use_quad == 0 || (p->use_quad < 0 && p->mk != MK_POP)) return false;
+    if (p->store != ST_F16 && p->store != ST_BF16) return false;
+    if (omega_out != nullptr || (pat != PAT_PULL && pat != PAT_AA_EVEN && pat != PAT_AA_ODD)) return false;
+    if (p->desc.dims[0] % 4 != 0) return false;
+    const size_t es = store_size(p->store);
+    if ((reinterpret_cast<uintptr_t>(src) + es) % (4 * es) != 0) return false;
+    if ((reinterpret_cast<uintptr_t>(dst) + es) % (4 * es) != 0) return false;
+    if (s[1] % 4 != 0 || s[2] % 4 != 0 || s[3] % 4 != 0) return false;
+    return quad_launcher(p, pat) != nullptr;
+}
 
 // The pair sweep needs an even row length, no omega output, and every row's interior cell x = 0
 // (ghost-inclusive x = 1) on a 2-element boundary so that paired loads / stores are aligned.
@@ -434,6 +462,8 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
     {
         const char* env = getenv("LBM_B200_PAIR");
         p->use_pair = env == nullptr ? -1 : (env[0] == '0' ? 0 : 1);
+        const char* qenv = getenv("LBM_B200_QUAD");
+        p->use_quad = qenv == nullptr ? -1 : (qenv[0] == '0' ? 0 : 1);
         const char* zenv = getenv("LBM_B200_ZC");
         p->zc = zenv != nullptr ? atoi(zenv) : 8;
         if (p->zc < 1) p->zc = 1;
@@ -522,7 +552,11 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
     }
     dim3 grid, block;
     SweepLauncher L;
-    if (pair_applicable(p, src, dst, strides, pat, omega_out)) {
+    if (quad_applicable(p, src, dst, strides, pat, omega_out)) {
+        L = quad_launcher(p, pat);
+        block = dim3(32, QUAD_ROWS, 1);
+        grid = dim3((a.g.nx + 127) / 128, (a.g.ny + QUAD_ROWS - 1) / QUAD_ROWS, a.g.nz);
+    } else if (pair_applicable(p, src, dst, strides, pat, omega_out)) {
         L = pair_launcher(p, pat);
         block = dim3(32, PAIR_ROWS, 1);
         grid = dim3((a.g.nx + 63) / 64, (a.g.ny + PAIR_ROWS - 1) / PAIR_ROWS, a.g.nz);

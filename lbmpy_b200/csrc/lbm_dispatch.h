@@ -2,7 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
-#include "lbm_pair.cuh"
+#include "lbm_quad.cuh"
 
 namespace lbm {
 
@@ -33,6 +33,22 @@ SweepLauncher pick_pair_pattern(int pat) {
         case PAT_PULL: return &launch_sweep_pair<S, Q, MK, PAT_PULL>;
         case PAT_AA_EVEN: return &launch_sweep_pair<S, Q, MK, PAT_AA_EVEN>;
         case PAT_AA_ODD: return &launch_sweep_pair<S, Q, MK, PAT_AA_ODD>;
+    }
+    return nullptr;
+}
+
+template <class S, int Q, int MK, int PAT>
+cudaError_t launch_sweep_quad(const SweepArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
+    k_sweep_quad<S, Q, MK, PAT><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S, int Q, int MK>
+SweepLauncher pick_quad_pattern(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_sweep_quad<S, Q, MK, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_sweep_quad<S, Q, MK, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_sweep_quad<S, Q, MK, PAT_AA_ODD>;
     }
     return nullptr;
 }
@@ -97,6 +113,13 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         if (store == ST_F32) return pick_batched_pattern<float, float, Q, MK>(pat);             \
         return nullptr;                                                                         \
     }                                                                                           \
+    SweepLauncher sweep_quad_##NAME(int store, int pat) {                                       \
+        switch (store) {                                                                        \
+            case ST_F16: return pick_quad_pattern<__half, Q, MK>(pat);                           \
+            case ST_BF16: return pick_quad_pattern<__nv_bfloat16, Q, MK>(pat);                  \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }                                                                                           \
     SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
         switch (store) {                                                                        \
             case ST_F32: return pick_pair_pattern<float, Q, MK>(pat);                            \
@@ -140,6 +163,7 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         if (store == ST_F32) return pick_batched_pattern<float, float, Q, MK>(pat);             \
         return nullptr;                                                                         \
     }                                                                                           \
+    SweepLauncher sweep_quad_##NAME(int, int) { return nullptr; }                               \
     SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
         if (store == ST_F32) return pick_pair_pattern<float, Q, MK>(pat);                       \
         return nullptr;                                                                         \
@@ -159,6 +183,7 @@ MacroLauncher pick_set_eq_pattern(int pat) {
     BatchLauncher batched_##NAME(int store, int pat);    \
     SweepLauncher sweep_##NAME(int store, int pat);      \
     SweepLauncher sweep_pair_##NAME(int store, int pat); \
+    SweepLauncher sweep_quad_##NAME(int store, int pat); \
     MacroLauncher set_eq_##NAME(int store, int pat);
 
 LBM_DECLARE_FAMILY(q19_pop)

@@ -88,8 +88,16 @@ constexpr int PAIR_ROWS = 4;
 
 // Requirements (checked by the host): nx even, the address of interior cell x = 0 of every row
 // and every slot 8-byte aligned for the paired type (x = 0 lands at an even element offset).
+// Resident blocks of 128 threads per SM the register allocation must allow.  16-bit storage:
+// the sweep is limited by latency rather than bandwidth at the occupancy its registers allow; a
+// cap of 80 registers (6 blocks) trades a few spilled words for a third more resident warps.
+// FP32: 5 blocks (at most 102 registers); without a stated minimum the allocator may take far more.
+template <class S> struct PairMinBlocks { static constexpr int value = 5; };
+template <> struct PairMinBlocks<__half> { static constexpr int value = 6; };
+template <> struct PairMinBlocks<__nv_bfloat16> { static constexpr int value = 6; };
+
 template <class S, int Q, int MK, int PAT>
-__global__ void __launch_bounds__(32 * PAIR_ROWS) k_sweep_pair(const SweepArgs a) {
+__global__ void __launch_bounds__(32 * PAIR_ROWS, PairMinBlocks<S>::value) k_sweep_pair(const SweepArgs a) {
     static_assert(PAT == PAT_PULL || PAT == PAT_AA_EVEN || PAT == PAT_AA_ODD, "pair sweep: pull and AA");
     using L = Lat<Q>;
     using A = Access<PAT>;

@@ -150,11 +150,12 @@ def test_sweep_parity(cuda, case, dtype, kernel, monkeypatch):
 
 
 @pytest.mark.parametrize("storage,bound", [("float16", 1e-3), ("bfloat16", 5e-3)])
-@pytest.mark.parametrize("kernel", ["pair", "cell"])
+@pytest.mark.parametrize("kernel", ["quad", "pair", "cell"])
 def test_low_precision_storage_l2_velocity(cuda, storage, bound, kernel, monkeypatch):
     """Zero-centred 16-bit storage with FP32 collision vs the FP64 oracle (TGV + noise).
     FP16 meets the 1e-3 bar; BF16's 8-bit mantissa leaves a few 1e-3 (bound stated per type)."""
     monkeypatch.setenv("LBM_B200_PAIR", "1" if kernel == "pair" else "0")
+    monkeypatch.setenv("LBM_B200_QUAD", "1" if kernel == "quad" else "0")
     n = (32, 32, 16)
     u = tgv_velocity(n, 0.04, noise=1e-3, seed=0)
     rho = np.ones(n)
@@ -242,3 +243,41 @@ def test_symbolic_relaxation_rate(cuda):
     assert pop_rel_linf(_interior(b), res[1:-1, 1:-1, 1:-1], k.method.weights) < 1e-13
     with pytest.raises(ValueError):
         k(src=a, dst=b)
+
+
+QUAD_CASES = [("d3q19-trt-aa-ldc", "D3Q19", "trt", "aa", (16, 12, 8), (0, 0, 0), "ldc",
+               dict(relaxation_rate=1.9, compressible=True)),
+              ("d3q19-trt-pull-periodic", "D3Q19", "trt", "pull", (20, 10, 6), (1, 1, 1), None,
+               dict(relaxation_rate=1.8, compressible=True, force=(1e-5, 0, 0))),
+              ("d3q27-cum-aa-channel", "D3Q27", "cumulant", "aa", (12, 10, 8), (1, 0, 0), "duct",
+               dict(relaxation_rate=1.95, compressible=True, galilean_correction=True, force=(1e-5, 0, 0))),
+              ("d3q19-srt-aa-periodic", "D3Q19", "srt", "aa", (8, 6, 6), (1, 1, 1), None,
+               dict(relaxation_rate=1.6, compressible=False))]
+
+
+@pytest.mark.parametrize("case", QUAD_CASES, ids=[c[0] for c in QUAD_CASES])
+@pytest.mark.parametrize("storage", ["float16", "bfloat16"])
+def test_quad_sweep_matches_pair_sweep(cuda, case, storage, monkeypatch):
+    """The four-cells-per-thread sweep against the two-cells-per-thread sweep on 16-bit storage
+    (the same packed FP32x2 collision, so the fields agree to the last 16-bit digit), 30 steps,
+    with walls, periodic wrap across the row ends and both AA parities."""
+    name, stencil, method, pattern, n, periodic, bkind, kw = case
+    fields = {}
+    for kernel in ("quad", "pair"):
+        monkeypatch.setenv("LBM_B200_PAIR", "1")
+        monkeypatch.setenv("LBM_B200_QUAD", "1" if kernel == "quad" else "0")
+        cfg = dict(stencil=getattr(L.Stencil, stencil), method=getattr(L.Method, method.upper()),
+                   streaming_pattern=pattern, **kw)
+        step = L.LatticeBoltzmannStep(domain_size=n, periodicity=periodic, optimization={"storage_dtype": storage},
+                                      config=L.CreateKernelConfig(data_type="float32"), **cfg)
+        for obj, sl in (_boundaries(bkind) or []):
+            step.boundary_handling.set_boundary(obj, sl)
+        step.velocity_array[...] = random_velocity(n, 2e-2, seed=3)
+        step.set_pdf_fields_from_macroscopic_values()
+        step.run(30)
+        fields[kernel] = _interior(step.pdfs)
+    fluid = np.ones(n, bool) if bkind is None else \
+        ((step.boundary_handling.flag_array & 7)[1:-1, 1:-1, 1:-1] == 0)
+    diff = np.abs(fields["quad"] - fields["pair"])[fluid].max()
+    scale = np.abs(fields["pair"][fluid]).max()
+    assert diff <= 1e-6 * scale, f"{name} {storage}: max difference {diff:.3e} (scale {scale:.3e})"
