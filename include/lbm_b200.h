@@ -90,6 +90,26 @@ int lbm_plan_update(LbmPlan* plan, const LbmPlanDesc* desc);
 int lbm_sweep(const LbmPlan* plan, const void* src, void* dst, const int64_t strides[4],
               const uint8_t* flags, int parity, float* omega_out, void* stream);
 
+/* Device status word of the plan, OR-ed by its sweeps since the last clear: 0 when every sweep
+ * ran to completion, LBM_STATUS_STAGE_TIMEOUT when a staged sweep gave up waiting for a
+ * shared-memory stage (its CTA left the rest of its cells un-updated).  Synchronises the device.
+ * lbmpy's generated kernels have no such word; it is the only way a sweep that must bound its
+ * waits reports that it stopped early.  clear != 0 resets it after reading. */
+#define LBM_STATUS_STAGE_TIMEOUT 1u
+int lbm_plan_status(LbmPlan* plan, uint32_t* status, int clear);
+
+/* Which kernel lbm_sweep runs for these arguments: one cell per thread, two or four x-adjacent
+ * cells per thread, or the row-staged sweep (shared-memory stages filled by bulk copies).  All
+ * give lbmpy's update; the choice follows storage type, method, alignment and the environment
+ * overrides LBM_B200_PAIR / LBM_B200_QUAD / LBM_B200_STAGED ("0" never, "1" when applicable).
+ * Diagnostic: lbmpy has one generated kernel per configuration and no such query. */
+#define LBM_VARIANT_CELL 0
+#define LBM_VARIANT_PAIR 1
+#define LBM_VARIANT_QUAD 2
+#define LBM_VARIANT_STAGED 3
+int lbm_sweep_variant(const LbmPlan* plan, const void* src, const void* dst, const int64_t strides[4],
+                      int parity, const float* omega_out, int* variant);
+
 /* Runs `steps` sweeps; for pull the fields alternate a->b->a..., for in-place patterns
  * `a` is updated starting at parity `first_parity`.  Sets *result_in_b for pull. */
 int lbm_run(const LbmPlan* plan, void* a, void* b, const int64_t strides[4], const uint8_t* flags,

@@ -17,10 +17,14 @@ DTYPE_F64, DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2, 3
 PATTERN_PULL, PATTERN_AA, PATTERN_ESOTWIST = 0, 1, 2
 FORCE_NONE, FORCE_GUO, FORCE_CENTRAL_MOMENT, FORCE_SIMPLE, FORCE_LUO = 0, 1, 2, 3, 4
 SGS_NONE, SGS_SMAGORINSKY, SGS_MLP = 0, 1, 2
+STATUS_STAGE_TIMEOUT = 1
+VARIANT_CELL, VARIANT_PAIR, VARIANT_QUAD, VARIANT_STAGED = 0, 1, 2, 3
+VARIANT_NAMES = {0: "cell", 1: "pair", 2: "quad", 3: "staged"}
 MLP_PARAMS = 1442
 
 # exported symbols, one per declaration in include/lbm_b200.h
-EXPORTS = ("lbm_plan_create", "lbm_plan_destroy", "lbm_plan_update", "lbm_sweep", "lbm_run",
+EXPORTS = ("lbm_plan_create", "lbm_plan_destroy", "lbm_plan_update", "lbm_plan_status", "lbm_sweep_variant",
+           "lbm_sweep", "lbm_run",
            "lbm_set_equilibrium", "lbm_get_macroscopic", "lbm_reduce_conserved", "lbm_reduce_conserved_noalloc",
            "lbm_flags_finalize", "lbm_closure_set_weights", "lbm_closure_features", "lbm_mlp_forward",
            "lbm_mlp_create", "lbm_mlp_destroy", "lbm_mlp_loss_grad", "lbm_mlp_adam", "lbm_batch_create", "lbm_batch_sweep", "lbm_batch_info", "lbm_batch_destroy",
@@ -78,6 +82,8 @@ def lib():
         L.lbm_plan_create.argtypes = [ctypes.POINTER(LbmPlanDesc), ctypes.POINTER(ctypes.c_void_p)]
         L.lbm_plan_destroy.argtypes = [vp]
         L.lbm_plan_update.argtypes = [vp, ctypes.POINTER(LbmPlanDesc)]
+        L.lbm_plan_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int]
+        L.lbm_sweep_variant.argtypes = [vp, vp, vp, i64p, ctypes.c_int, vp, ctypes.POINTER(ctypes.c_int)]
         L.lbm_sweep.argtypes = [vp, vp, vp, i64p, vp, ctypes.c_int, vp, vp]
         L.lbm_run.argtypes = [vp, vp, vp, i64p, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp]
         L.lbm_set_equilibrium.argtypes = [vp, vp, i64p, vp, i64p, vp, i64p, ctypes.c_int, vp]
@@ -142,6 +148,12 @@ class Plan:
     def update(self, desc: LbmPlanDesc):
         check(lib().lbm_plan_update(self.handle, ctypes.byref(desc)), "lbm_plan_update")
         self.desc = desc
+
+    def status(self, clear: bool = True) -> int:
+        """Device status word OR-ed by the plan's sweeps (0: every sweep completed)."""
+        v = ctypes.c_uint32(0)
+        check(lib().lbm_plan_status(self.handle, ctypes.byref(v), int(clear)), "lbm_plan_status")
+        return v.value
 
     def __del__(self):
         h = getattr(self, "handle", None)

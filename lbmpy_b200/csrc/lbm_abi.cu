@@ -25,6 +25,10 @@ struct LbmPlan {
     int use_pair;          // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_PAIR)
     int zc;                // z-planes per thread of the FP32 closure sweep (environment LBM_B200_ZC, else 8)
     int use_quad;          // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_QUAD)
+    int use_staged;        // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_STAGED)
+    int ns;                // shared-memory stages of the staged sweep (environment LBM_B200_NS, else 2)
+    int sms;               // multiprocessors of the plan's device
+    unsigned* status;      // device status word (lbm_plan_status), inside the reduction scratch
     void* ubb_rho;         // compressible + moving UBB walls: density gathered before the sweep
     Physics phys;
     double* partial;       // reduction scratch: RED_BLOCKS * 5 doubles
@@ -202,6 +206,34 @@ bool pair_applicable(const LbmPlan* p, const void* src, const void* dst, const i
     if ((reinterpret_cast<uintptr_t>(dst) + es) % (2 * es) != 0) return false;
     if (s[1] % 2 != 0 || s[2] % 2 != 0 || s[3] % 2 != 0) return false;
     return pair_launcher(p, pat) != nullptr;
+}
+
+StagedLauncher staged_launcher(const LbmPlan* p, int pat) {
+    if (p->q == 19 && p->mk == MK_POP) return sweep_staged_q19_pop(p->store, pat);
+    if (p->q == 19 && p->mk == MK_MRT) return sweep_staged_q19_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_POP) return sweep_staged_q27_pop(p->store, pat);
+    if (p->q == 27 && p->mk == MK_MRT) return sweep_staged_q27_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM) return sweep_staged_q27_cum(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM1) return sweep_staged_q27_cum1(p->store, pat);
+    return nullptr;
+}
+
+// The staged sweep copies row segments in 16-byte chunks: the source rows of every slot must
+// start (interior cell x = 0) on a 16-byte boundary, the y / z / slot strides and the row length
+// must be whole 16-byte units.  The tile count must fit an int.
+bool staged_applicable(const LbmPlan* p, const void* src, const int64_t s[4], int pat) {
+    if (p->use_staged <= 0) return false;
+    if (pat != PAT_PULL && pat != PAT_AA_EVEN && pat != PAT_AA_ODD) return false;
+    const size_t es = store_size(p->store);
+    if (size_t(p->desc.dims[0]) * es % 16 != 0) return false;
+    if ((reinterpret_cast<uintptr_t>(src) + es * size_t(1 + s[1] + s[2])) % 16 != 0) return false;
+    if (size_t(s[1]) * es % 16 != 0 || size_t(s[2]) * es % 16 != 0 || size_t(s[3]) * es % 16 != 0) return false;
+    // 16-bit storage copies the halo element after a row's ghost cell as a 4-byte word with its
+    // successor, which must lie in the row's padding
+    if (es == 2 && s[1] < int64_t(p->desc.dims[0]) + 3) return false;
+    const long long tiles = (long long)((p->desc.dims[0] + 31) / 32) * p->desc.dims[1] * p->desc.dims[2];
+    if (tiles > 0x7fffffffLL) return false;
+    return staged_launcher(p, pat) != nullptr;
 }
 
 MacroLauncher set_eq_launcher(const LbmPlan* p, int pat) {
@@ -467,14 +499,24 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
         const char* zenv = getenv("LBM_B200_ZC");
         p->zc = zenv != nullptr ? atoi(zenv) : 8;
         if (p->zc < 1) p->zc = 1;
+        const char* senv = getenv("LBM_B200_STAGED");
+        p->use_staged = senv == nullptr ? -1 : (senv[0] == '0' ? 0 : 1);
+        const char* nenv = getenv("LBM_B200_NS");
+        p->ns = nenv != nullptr ? atoi(nenv) : 2;
+        if (p->ns < 2) p->ns = 2;
+        if (p->ns > STAGED_MAX_NS) p->ns = STAGED_MAX_NS;
     }
     fill_physics(p, desc);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
+    p->sms = sms;
     p->red_blocks = sms * 4;
-    e = cudaMalloc(&p->partial, sizeof(double) * 5 * (p->red_blocks + 1));
+    e = cudaMalloc(&p->partial, sizeof(double) * (5 * (p->red_blocks + 1) + 1));
     if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaMalloc(reduction scratch)"); }
     p->red_out = p->partial + 5 * p->red_blocks;
+    p->status = reinterpret_cast<unsigned*>(p->partial + 5 * (p->red_blocks + 1));
+    e = cudaMemset(p->status, 0, sizeof(double));
+    if (e != cudaSuccess) { cudaFree(p->partial); delete p; return cuda_fail(e, "cudaMemset(status)"); }
     p->ubb_rho = nullptr;
     if (sweep_launcher(p, PAT_PULL) == nullptr) {
         cudaFree(p->partial);
@@ -528,6 +570,15 @@ static int validate_sweep(const LbmPlan* p, const void* src, const void* dst, co
     return LBM_OK;
 }
 
+// Which sweep kernel a launch with these arguments uses (LBM_VARIANT_*), in order of preference.
+static int sweep_variant(const LbmPlan* p, const void* src, const void* dst, const int64_t strides[4], int pat,
+                         const float* omega_out) {
+    if (staged_applicable(p, src, strides, pat)) return LBM_VARIANT_STAGED;
+    if (quad_applicable(p, src, dst, strides, pat, omega_out)) return LBM_VARIANT_QUAD;
+    if (pair_applicable(p, src, dst, strides, pat, omega_out)) return LBM_VARIANT_PAIR;
+    return LBM_VARIANT_CELL;
+}
+
 // Launch without re-validating (arguments checked by the caller).
 static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, const int64_t strides[4],
                                 const uint8_t* flags, int parity, float* omega_out, cudaStream_t stream) {
@@ -541,6 +592,7 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
     a.zc = (p->mk == MK_CUM1_MLP && p->store == ST_F32) ? p->zc : 1;
     a.pad_ = 0;
     a.ubb_rho = nullptr;
+    a.status = p->status;
     if (flags != nullptr && p->ubb_rho != nullptr && needs_ubb_density(&p->desc)) {
         UbbLauncher U = p->q == 19 ? ubb_launcher_q<19>(p->store, pat) : ubb_launcher_q<27>(p->store, pat);
         if (U == nullptr) return fail(LBM_E_UNSUPPORTED, "no wall-density kernel for this storage type / pattern");
@@ -550,13 +602,20 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
         if (e != cudaSuccess) return cuda_fail(e, "wall-density launch");
         a.ubb_rho = p->ubb_rho;
     }
+    const int variant = sweep_variant(p, src, dst, strides, pat, omega_out);
+    if (variant == LBM_VARIANT_STAGED) {
+        StagedLauncher SL = staged_launcher(p, pat);
+        cudaError_t e = SL(a, p->ns, p->sms, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "staged sweep launch");
+        return LBM_OK;
+    }
     dim3 grid, block;
     SweepLauncher L;
-    if (quad_applicable(p, src, dst, strides, pat, omega_out)) {
+    if (variant == LBM_VARIANT_QUAD) {
         L = quad_launcher(p, pat);
         block = dim3(32, QUAD_ROWS, 1);
         grid = dim3((a.g.nx + 127) / 128, (a.g.ny + QUAD_ROWS - 1) / QUAD_ROWS, a.g.nz);
-    } else if (pair_applicable(p, src, dst, strides, pat, omega_out)) {
+    } else if (variant == LBM_VARIANT_PAIR) {
         L = pair_launcher(p, pat);
         block = dim3(32, PAIR_ROWS, 1);
         grid = dim3((a.g.nx + 63) / 64, (a.g.ny + PAIR_ROWS - 1) / PAIR_ROWS, a.g.nz);
@@ -576,6 +635,31 @@ int lbm_sweep(const LbmPlan* p, const void* src, void* dst, const int64_t stride
     if (rc) return rc;
     if (parity != 0 && parity != 1) return fail(LBM_E_INVALID, "parity must be 0 (EVEN) or 1 (ODD)");
     return launch_sweep_checked(p, src, dst, strides, flags, parity, omega_out, static_cast<cudaStream_t>(stream));
+}
+
+int lbm_sweep_variant(const LbmPlan* p, const void* src, const void* dst, const int64_t strides[4], int parity,
+                      const float* omega_out, int* variant) {
+    if (variant == nullptr) return fail(LBM_E_INVALID, "variant must not be NULL");
+    int rc = validate_sweep(p, src, dst, strides, nullptr, omega_out);
+    if (rc) return rc;
+    if (parity != 0 && parity != 1) return fail(LBM_E_INVALID, "parity must be 0 (EVEN) or 1 (ODD)");
+    *variant = sweep_variant(p, src, dst, strides, pattern_kind(p, parity), omega_out);
+    return LBM_OK;
+}
+
+int lbm_plan_status(LbmPlan* p, uint32_t* status, int clear) {
+    if (p == nullptr || status == nullptr) return fail(LBM_E_INVALID, "plan and status must not be NULL");
+    int rc = check_device(p);
+    if (rc) return rc;
+    unsigned v = 0;
+    cudaError_t e = cudaMemcpy(&v, p->status, sizeof(v), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "reading the plan status");
+    if (clear) {
+        e = cudaMemset(p->status, 0, sizeof(unsigned));
+        if (e != cudaSuccess) return cuda_fail(e, "clearing the plan status");
+    }
+    *status = v;
+    return LBM_OK;
 }
 
 int lbm_run(const LbmPlan* p, void* a, void* b, const int64_t strides[4], const uint8_t* flags, int first_parity,

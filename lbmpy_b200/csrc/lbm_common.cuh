@@ -117,6 +117,7 @@ struct SweepArgs {
     int zc;                // closure sweep: consecutive z-planes per thread (next plane prefetched to L2)
     int pad_;
     const void* ubb_rho;   // compressible moving walls: previous-step density of the cells next to them
+    unsigned* status;      // device status word of the plan (STATUS_* bits), or nullptr
 };
 
 // Neighbour offsets in elements for c in {-1, 0, +1} along each axis, with periodic wrap.

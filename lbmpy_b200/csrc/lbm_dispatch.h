@@ -2,7 +2,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "lbm_quad.cuh"
+#include "lbm_staged.cuh"
 
 namespace lbm {
 
@@ -49,6 +52,50 @@ SweepLauncher pick_quad_pattern(int pat) {
         case PAT_PULL: return &launch_sweep_quad<S, Q, MK, PAT_PULL>;
         case PAT_AA_EVEN: return &launch_sweep_quad<S, Q, MK, PAT_AA_EVEN>;
         case PAT_AA_ODD: return &launch_sweep_quad<S, Q, MK, PAT_AA_ODD>;
+    }
+    return nullptr;
+}
+
+// Staged sweep: the launcher sizes the persistent grid itself (resident CTAs per SM x SMs, at
+// most one CTA per tile).  W = cells per tile = threads per CTA.
+using StagedLauncher = cudaError_t (*)(const SweepArgs&, int ns, int sms, cudaStream_t);
+
+template <class S> struct StagedWidth { static constexpr int value = 128; };
+template <> struct StagedWidth<double> { static constexpr int value = 128; };
+
+template <class S, class R, int Q, int MK, int PAT>
+cudaError_t launch_sweep_staged(const SweepArgs& a, int ns, int sms, cudaStream_t s) {
+    constexpr int W = StagedWidth<S>::value;
+    using Lay = StagedLayout<S, Q, W>;
+    if (ns < 2 || ns > STAGED_MAX_NS) return cudaErrorInvalidValue;
+    auto kern = &k_sweep_staged<S, R, Q, MK, PAT, W>;
+    const size_t smem = Lay::smem_bytes(ns);
+    // resident CTAs per SM for the last stage count asked for, packed as ns << 8 | blocks
+    static std::atomic<int> cached{0};
+    const int c = cached.load(std::memory_order_relaxed);
+    int per_sm = c & 255;
+    if ((c >> 8) != ns) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W, smem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        per_sm = per_sm > 255 ? 255 : per_sm;
+        cached.store((ns << 8) | per_sm, std::memory_order_relaxed);
+    }
+    const long long tiles = (long long)((a.g.nx + W - 1) / W) * a.g.ny * a.g.nz;
+    const long long slots = (long long)per_sm * sms;
+    const unsigned grid = (unsigned)(tiles < slots ? tiles : slots);
+    kern<<<grid, W, smem, s>>>(a, ns);
+    return cudaGetLastError();
+}
+
+template <class S, class R, int Q, int MK>
+StagedLauncher pick_staged_pattern(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_sweep_staged<S, R, Q, MK, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_sweep_staged<S, R, Q, MK, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_sweep_staged<S, R, Q, MK, PAT_AA_ODD>;
     }
     return nullptr;
 }
@@ -120,6 +167,15 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         }                                                                                       \
         return nullptr;                                                                         \
     }                                                                                           \
+    StagedLauncher sweep_staged_##NAME(int store, int pat) {                                    \
+        switch (store) {                                                                        \
+            case ST_F64: return pick_staged_pattern<double, double, Q, MK>(pat);                 \
+            case ST_F32: return pick_staged_pattern<float, float, Q, MK>(pat);                   \
+            case ST_F16: return pick_staged_pattern<__half, float, Q, MK>(pat);                  \
+            case ST_BF16: return pick_staged_pattern<__nv_bfloat16, float, Q, MK>(pat);         \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }                                                                                           \
     SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
         switch (store) {                                                                        \
             case ST_F32: return pick_pair_pattern<float, Q, MK>(pat);                            \
@@ -164,6 +220,11 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         return nullptr;                                                                         \
     }                                                                                           \
     SweepLauncher sweep_quad_##NAME(int, int) { return nullptr; }                               \
+    StagedLauncher sweep_staged_##NAME(int store, int pat) {                                    \
+        if (store == ST_F64) return pick_staged_pattern<double, double, Q, MK>(pat);            \
+        if (store == ST_F32) return pick_staged_pattern<float, float, Q, MK>(pat);              \
+        return nullptr;                                                                         \
+    }                                                                                           \
     SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
         if (store == ST_F32) return pick_pair_pattern<float, Q, MK>(pat);                       \
         return nullptr;                                                                         \
@@ -184,6 +245,7 @@ MacroLauncher pick_set_eq_pattern(int pat) {
     SweepLauncher sweep_##NAME(int store, int pat);      \
     SweepLauncher sweep_pair_##NAME(int store, int pat); \
     SweepLauncher sweep_quad_##NAME(int store, int pat); \
+    StagedLauncher sweep_staged_##NAME(int store, int pat); \
     MacroLauncher set_eq_##NAME(int store, int pat);
 
 LBM_DECLARE_FAMILY(q19_pop)

@@ -138,6 +138,14 @@ class BoundSweep:
         if rc:
             N.check(rc, "lbm_sweep")
 
+    def variant(self, src_ptr: int, dst_ptr: int, parity: int) -> str:
+        """Name of the sweep kernel a launch with these fields uses ("cell", "pair", "quad",
+        "staged")."""
+        v = ctypes.c_int(-1)
+        N.check(self._lib.lbm_sweep_variant(self.plan.handle, ctypes.c_void_p(src_ptr), ctypes.c_void_p(dst_ptr),
+                                            self._strides, parity, None, ctypes.byref(v)), "lbm_sweep_variant")
+        return N.VARIANT_NAMES[v.value]
+
     def run(self, a_ptr: int, b_ptr: int, first_parity: int, steps: int) -> bool:
         """`steps` sweeps in one call; returns True if a pull result ended in `b`."""
         in_b = ctypes.c_int(0)
@@ -171,6 +179,14 @@ class LbKernel:
         elif bytes(p.desc) != bytes(desc):
             p.update(desc)
         return p
+
+    def status(self, clear: bool = True) -> int:
+        """OR of the device status words of every plan of this kernel (0: every sweep ran to
+        completion; N.STATUS_STAGE_TIMEOUT: a staged sweep stopped waiting for its data)."""
+        v = 0
+        for p in self._plans.values():
+            v |= p.status(clear)
+        return v
 
     def bind(self, pdfs: torch.Tensor, periodic, flags=None, ubb_velocities=None, params=None,
              stream=None) -> BoundSweep:

@@ -178,6 +178,23 @@ class LatticeBoltzmannStep:
     def previous_timestep(self):
         return self._prev
 
+    def sweep_variant(self) -> str:
+        """Name of the kernel the next sweep runs ("cell", "pair", "quad" or "staged")."""
+        b = self._bound()
+        if self._inplace:
+            p = self.pdfs.data_ptr()
+            return b.variant(p, p, int(self._prev.next().idx))
+        return b.variant(self.pdfs.data_ptr(), self.pdfs_tmp.data_ptr(), 0)
+
+    def sweep_status(self, clear: bool = True) -> int:
+        """Device status of the sweeps run so far (synchronises): 0 when every sweep ran to
+        completion, else the STATUS_* bits of lbmpy_b200._native (a staged sweep that gave up
+        waiting for its data leaves its remaining cells un-updated and sets a bit)."""
+        v = 0
+        for k in self._kernels:
+            v |= k.status(clear)
+        return v
+
     # ------------------------------------------------------------------------------ running
     def _flags(self, kernel):
         if not self._boundary_handling.has_boundaries:
