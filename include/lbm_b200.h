@@ -148,7 +148,10 @@ int lbm_reduce_conserved_noalloc(const LbmPlanDesc* desc, const void* pdfs, cons
 
 /* Sets bit 7 on every fluid cell of `flags` (device, layout above) that has a boundary
  * neighbour along the plan's stencil, honouring periodicity.  Replaces the link-list setup of
- * LatticeBoltzmannBoundaryHandling (boundaries/boundaryhandling.py:15-155). */
+ * LatticeBoltzmannBoundaryHandling (boundaries/boundaryhandling.py:15-155).
+ * It also records, in the plan, which interior rows (y, z) hold a non-zero flag; the plan's
+ * sweeps given this same `flags` pointer skip the flag loads of the other rows.  Call it again
+ * (with every plan that sweeps the field) after changing the field's contents. */
 int lbm_flags_finalize(const LbmPlan* plan, uint8_t* flags, void* stream);
 
 /* ---- Learned eddy-viscosity closure ----

@@ -29,6 +29,8 @@ struct LbmPlan {
     int ns;                // shared-memory stages of the staged sweep (environment LBM_B200_NS, else 2)
     int sms;               // multiprocessors of the plan's device
     unsigned* status;      // device status word (lbm_plan_status), inside the reduction scratch
+    uint32_t* rowmask;     // row summary of the flag field last finalized with this plan
+    mutable const uint8_t* rowmask_flags;  // that flag field (sweeps given it use the summary)
     void* ubb_rho;         // compressible + moving UBB walls: density gathered before the sweep
     Physics phys;
     double* partial;       // reduction scratch: RED_BLOCKS * 5 doubles
@@ -110,6 +112,7 @@ Grid make_grid(const LbmPlan* p, const int64_t s[4], const uint8_t* flags) {
     g.flags = flags;
     g.fsy = g.nx + 2;
     g.fsz = (g.nx + 2) * (g.ny + 2);
+    g.rowmask = nullptr;
     return g;
 }
 
@@ -157,6 +160,10 @@ SweepLauncher pair_launcher(const LbmPlan* p, int pat) {
 }
 
 size_t store_size(int store) { return store == ST_F64 ? 8 : (store == ST_F32 ? 4 : 2); }
+
+size_t rowmask_bytes(const LbmPlan* p) {
+    return sizeof(uint32_t) * ((size_t(p->desc.dims[1]) * p->desc.dims[2] + 31) / 32);
+}
 
 SweepLauncher quad_launcher(const LbmPlan* p, int pat) {
     if (p->q == 19 && p->mk == MK_POP) return sweep_quad_q19_pop(p->store, pat);
@@ -359,6 +366,19 @@ int ensure_ubb_buffer(LbmPlan* p) {
     return LBM_OK;
 }
 
+// Row summary of a finalized flag field: bit y + ny*z for every interior row with a non-zero flag.
+__global__ void k_row_mask(Grid g, uint32_t* mask) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.ny * g.nz) return;
+    const int y = r % g.ny, z = r / g.ny;
+    const uint8_t* row = g.flags + 1 + (y + 1) * g.fsy + (z + 1) * g.fsz;
+    for (int x = 0; x < g.nx; ++x)
+        if (row[x] != 0) {
+            atomicOr(mask + (r >> 5), 1u << (r & 31));
+            break;
+        }
+}
+
 // Marks fluid cells that have a boundary neighbour along the stencil.
 template <int Q>
 __global__ void k_flags_finalize(Grid g) {
@@ -518,6 +538,8 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
     e = cudaMemset(p->status, 0, sizeof(double));
     if (e != cudaSuccess) { cudaFree(p->partial); delete p; return cuda_fail(e, "cudaMemset(status)"); }
     p->ubb_rho = nullptr;
+    p->rowmask = nullptr;
+    p->rowmask_flags = nullptr;
     if (sweep_launcher(p, PAT_PULL) == nullptr) {
         cudaFree(p->partial);
         delete p;
@@ -527,6 +549,13 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
         cudaFree(p->partial);
         delete p;
         return rc2;
+    }
+    e = cudaMalloc(&p->rowmask, rowmask_bytes(p));
+    if (e != cudaSuccess) {
+        cudaFree(p->partial);
+        if (p->ubb_rho) cudaFree(p->ubb_rho);
+        delete p;
+        return cuda_fail(e, "cudaMalloc(row summary)");
     }
     *out = p;
     return LBM_OK;
@@ -550,6 +579,7 @@ int lbm_plan_destroy(LbmPlan* p) {
     if (p == nullptr) return LBM_OK;
     if (p->partial) cudaFree(p->partial);
     if (p->ubb_rho) cudaFree(p->ubb_rho);
+    if (p->rowmask) cudaFree(p->rowmask);
     delete p;
     return LBM_OK;
 }
@@ -593,6 +623,7 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
     a.pad_ = 0;
     a.ubb_rho = nullptr;
     a.status = p->status;
+    if (flags != nullptr && flags == p->rowmask_flags) a.g.rowmask = p->rowmask;
     if (flags != nullptr && p->ubb_rho != nullptr && needs_ubb_density(&p->desc)) {
         UbbLauncher U = p->q == 19 ? ubb_launcher_q<19>(p->store, pat) : ubb_launcher_q<27>(p->store, pat);
         if (U == nullptr) return fail(LBM_E_UNSUPPORTED, "no wall-density kernel for this storage type / pattern");
@@ -783,7 +814,17 @@ int lbm_flags_finalize(const LbmPlan* p, uint8_t* flags, void* stream) {
     if (p->q == 19) k_flags_finalize<19><<<grid, block, 0, st>>>(g);
     else k_flags_finalize<27><<<grid, block, 0, st>>>(g);
     cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "flag finalize launch");
+    if (e != cudaSuccess) return cuda_fail(e, "flag finalize launch");
+    // the row summary the sweeps of this plan use with this flag field
+    p->rowmask_flags = nullptr;
+    e = cudaMemsetAsync(p->rowmask, 0, rowmask_bytes(p), st);
+    if (e != cudaSuccess) return cuda_fail(e, "clearing the row summary");
+    const int rows = g.ny * g.nz;
+    k_row_mask<<<(rows + 255) / 256, 256, 0, st>>>(g, p->rowmask);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "row summary launch");
+    p->rowmask_flags = flags;
+    return LBM_OK;
 }
 
 }  // extern "C"

@@ -106,6 +106,10 @@ struct Grid {
     int periodic;          // bit 0 x, bit 1 y, bit 2 z
     const uint8_t* flags;  // (nx+2)*(ny+2)*(nz+2), x fastest, or nullptr
     int fsy, fsz;          // flag strides
+    // Bit y + ny*z set: interior row (y, z) holds a cell whose flag is non-zero (a boundary cell
+    // or a fluid cell next to one).  nullptr: every row may.  Sweeps skip the flag loads of the
+    // other rows, so that a fluid cell's populations are not held up behind its flag.
+    const uint32_t* rowmask;
 };
 
 struct SweepArgs {
@@ -119,6 +123,13 @@ struct SweepArgs {
     const void* ubb_rho;   // compressible moving walls: previous-step density of the cells next to them
     unsigned* status;      // device status word of the plan (STATUS_* bits), or nullptr
 };
+
+// Whether interior row (y, z) may hold a cell with a non-zero flag.
+__device__ __forceinline__ bool row_flagged(const Grid& g, int y, int z) {
+    if (g.rowmask == nullptr) return true;
+    const unsigned r = unsigned(y) + unsigned(g.ny) * unsigned(z);
+    return (__ldg(g.rowmask + (r >> 5)) >> (r & 31u)) & 1u;
+}
 
 // Neighbour offsets in elements for c in {-1, 0, +1} along each axis, with periodic wrap.
 struct NbrOffsets {

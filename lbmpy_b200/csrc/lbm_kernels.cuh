@@ -120,7 +120,7 @@ __device__ __forceinline__ void sweep_cell(const SweepArgs& a, int x, int y, int
     // before its loads issue.  The specialised cumulant sweep keeps the flag first: its register
     // budget (64 per thread for AA) does not hold the flag alongside 27 loads in flight.
     constexpr bool flag_first = MK == MK_CUM1 || MK == MK_CUM1_MLP;
-    const int fl = g.flags != nullptr ? g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz] : 0;
+    const int fl = (g.flags != nullptr && row_flagged(g, y, z)) ? g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz] : 0;
     if (flag_first && (fl & FLAG_TYPE_MASK)) return;
     NbrOffsets nb;
     nb.init(g, x, y, z);

@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(32 * PAIR_ROWS, PairMinBlocks<S>::value) k_swe
     S* dst = static_cast<S*>(a.dst);
 
     int flA = 0, flB = 0;
-    if (g.flags != nullptr) {
+    if (g.flags != nullptr && row_flagged(g, y, z)) {
         const int fc = (x0 + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz;
         flA = g.flags[fc];
         flB = g.flags[fc + 1];

@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(256) k_sweep_closure_tc(const SweepArgs a) {
 #pragma unroll 1
     for (int z = z0; z < z1; ++z) {
         if (z + 1 < z1) prefetch_cell<float, 27, PAT>(a, x, y, z + 1);
-        const int fl = g.flags != nullptr ? g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz] : 0;
+        const int fl = (g.flags != nullptr && row_flagged(g, y, z)) ? g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz] : 0;
         NbrOffsets nb;
         nb.init(g, x, y, z);
         const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;

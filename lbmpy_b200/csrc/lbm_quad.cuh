@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(32 * QUAD_ROWS, 4) k_sweep_quad(const SweepArg
     S* dst = static_cast<S*>(a.dst);
 
     int fl[4] = {0, 0, 0, 0};
-    if (g.flags != nullptr) {
+    if (g.flags != nullptr && row_flagged(g, y, z)) {
         const int fc = (x0 + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz;
 #pragma unroll
         for (int k = 0; k < 4; ++k) fl[k] = g.flags[fc + k];

@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(W) k_sweep_staged(const SweepArgs a, const int
         staged::arrive(bar);
     };
     auto flag_of = [&](const StagedTile& t) -> int {
-        if (g.flags == nullptr || tid >= t.w) return 0;
+        if (g.flags == nullptr || tid >= t.w || !row_flagged(g, t.y, t.z)) return 0;
         return g.flags[(t.xs + tid + 1) + (t.y + 1) * g.fsy + (t.z + 1) * g.fsz];
     };
 
