@@ -36,7 +36,7 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per sweep launch from one ncu capture of the same workload, averaged
 # over the launches captured; summaries with their commands are under profiles/.
 NCU_TRAFFIC_BYTES = {
-    "d3q27-cumulant-aa-channel-256x128x128": 876_794_112,   # k_sweep_d3q27_cumulant_aa_channel_256x128x128.md
+    "d3q27-cumulant-aa-channel-256x128x128": 875_081_216,   # k_sweep_d3q27_cumulant_aa_channel_256x128x128.md
     "d3q19-trt-pull-float32-256": 2_547_412_000,            # k_sweep_d3q19_fp32_fp16_256.md
     "d3q19-mrt-pull-float32-256": 2_550_143_000,
     "d3q19-trt-pull-float16-256": 1_276_317_824,             # k_sweep_quad_d3q19_trt_pull_fp16_256.md

@@ -128,7 +128,7 @@ struct SweepArgs {
 __device__ __forceinline__ bool row_flagged(const Grid& g, int y, int z) {
     if (g.rowmask == nullptr) return true;
     const unsigned r = unsigned(y) + unsigned(g.ny) * unsigned(z);
-    return (__ldg(g.rowmask + (r >> 5)) >> (r & 31u)) & 1u;
+    return (g.rowmask[r >> 5] >> (r & 31u)) & 1u;
 }
 
 // Neighbour offsets in elements for c in {-1, 0, +1} along each axis, with periodic wrap.
