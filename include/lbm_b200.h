@@ -40,7 +40,10 @@ enum {
 enum { LBM_STENCIL_D3Q19 = 19, LBM_STENCIL_D3Q27 = 27 };
 enum { LBM_METHOD_SRT = 0, LBM_METHOD_TRT = 1, LBM_METHOD_MRT = 2, LBM_METHOD_CUMULANT = 3 };
 enum { LBM_DTYPE_F64 = 0, LBM_DTYPE_F32 = 1, LBM_DTYPE_F16 = 2, LBM_DTYPE_BF16 = 3 };
-enum { LBM_PATTERN_PULL = 0, LBM_PATTERN_AA = 1, LBM_PATTERN_ESOTWIST = 2 };
+/* pull / push: two fields; AA, EsoTwist, EsoPull, EsoPush: in place (fieldaccess.py:66-318).
+ * Push, EsoPull and EsoPush are built for FP64 / FP32 storage. */
+enum { LBM_PATTERN_PULL = 0, LBM_PATTERN_AA = 1, LBM_PATTERN_ESOTWIST = 2, LBM_PATTERN_PUSH = 3,
+       LBM_PATTERN_ESOPULL = 4, LBM_PATTERN_ESOPUSH = 5 };
 enum { LBM_FORCE_NONE = 0, LBM_FORCE_GUO = 1, LBM_FORCE_CENTRAL_MOMENT = 2, LBM_FORCE_SIMPLE = 3,
        LBM_FORCE_LUO = 4 };
 enum { LBM_SGS_NONE = 0, LBM_SGS_SMAGORINSKY = 1, LBM_SGS_MLP = 2 };
@@ -84,8 +87,9 @@ int lbm_plan_update(LbmPlan* plan, const LbmPlanDesc* desc);
  * (creationfunctions.py:543-559), called as kernel(src=..., dst=...) by
  * LatticeBoltzmannStep.time_step (lbstep.py:271-282), together with the boundary handling
  * (boundaries/boundaryhandling.py:15-155) and periodic synchronisation it runs before the
- * sweep.  Two-field pull: src != dst.  In-place AA / EsoTwist: src == dst and `parity` is the
- * parity of THIS step (0 = EVEN, 1 = ODD; advanced_streaming/utility.py:18-38).
+ * sweep.  Two-field pull / push: src != dst.  In-place AA / EsoTwist / EsoPull / EsoPush:
+ * src == dst and `parity` is the parity of THIS step (0 = EVEN, 1 = ODD;
+ * advanced_streaming/utility.py:18-38).
  * omega_out (optional, float32, nx*ny*nz x-fastest) receives the effective shear rate. */
 int lbm_sweep(const LbmPlan* plan, const void* src, void* dst, const int64_t strides[4],
               const uint8_t* flags, int parity, float* omega_out, void* stream);
@@ -110,7 +114,7 @@ int lbm_plan_status(LbmPlan* plan, uint32_t* status, int clear);
 int lbm_sweep_variant(const LbmPlan* plan, const void* src, const void* dst, const int64_t strides[4],
                       int parity, const float* omega_out, int* variant);
 
-/* Runs `steps` sweeps; for pull the fields alternate a->b->a..., for in-place patterns
+/* Runs `steps` sweeps; for pull / push the fields alternate a->b->a..., for in-place patterns
  * `a` is updated starting at parity `first_parity`.  Sets *result_in_b for pull. */
 int lbm_run(const LbmPlan* plan, void* a, void* b, const int64_t strides[4], const uint8_t* flags,
             int first_parity, int steps, int* result_in_b, void* stream);

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "liblbmb200.so")
 LBM_OK, LBM_E_INVALID, LBM_E_CUDA, LBM_E_UNSUPPORTED, LBM_E_DEVICE = 0, 1, 2, 3, 4
 METHOD_SRT, METHOD_TRT, METHOD_MRT, METHOD_CUMULANT = 0, 1, 2, 3
 DTYPE_F64, DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2, 3
-PATTERN_PULL, PATTERN_AA, PATTERN_ESOTWIST = 0, 1, 2
+PATTERN_PULL, PATTERN_AA, PATTERN_ESOTWIST, PATTERN_PUSH, PATTERN_ESOPULL, PATTERN_ESOPUSH = 0, 1, 2, 3, 4, 5
 FORCE_NONE, FORCE_GUO, FORCE_CENTRAL_MOMENT, FORCE_SIMPLE, FORCE_LUO = 0, 1, 2, 3, 4
 SGS_NONE, SGS_SMAGORINSKY, SGS_MLP = 0, 1, 2
 STATUS_STAGE_TIMEOUT = 1

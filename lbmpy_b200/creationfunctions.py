@@ -457,8 +457,9 @@ def create_lb_update_rule(collision_rule=None, lbm_config=None, lbm_optimisation
         raise NotImplementedError(f"kernel_type {lbm_config.kernel_type!r} is not built; the fused "
                                   "stream-collide sweep is")
     pattern = lbm_config.streaming_pattern
-    if pattern not in ("pull", "aa", "esotwist"):
-        raise NotImplementedError(f"streaming pattern {pattern!r} is not built (pull, aa and esotwist are)")
+    if pattern not in ("pull", "push", "aa", "esotwist", "esopull", "esopush"):
+        raise NotImplementedError(f"streaming pattern {pattern!r} is not built (pull, push, aa, esotwist, "
+                                  "esopull and esopush are)")
     if is_inplace(pattern) and lbm_config.timestep == Timestep.BOTH:
         raise ValueError(f"Invalid timestep for streaming pattern {pattern}: Both")
     if lbm_optimisation.field_layout not in ("fzyx", "f", "reverse_numpy", "SoA"):
@@ -474,6 +475,8 @@ def create_lb_update_rule(collision_rule=None, lbm_config=None, lbm_optimisation
         raise ValueError("16-bit PDF storage collides in float32: set data_type='float32'")
     if storage == "float64" and data_type != "float64" or storage == "float32" and data_type != "float32":
         raise ValueError("storage_dtype must match data_type unless it is a 16-bit type")
+    if storage in ("float16", "bfloat16") and pattern in ("push", "esopull", "esopush"):
+        raise NotImplementedError(f"streaming pattern {pattern!r} is built for float64 / float32 storage")
     rule = LbmUpdateRule(collision_rule, pattern, lbm_config.timestep, lbm_config.field_name,
                          lbm_config.temporary_field_name, data_type, storage,
                          tuple(bool(b) for b in (list(lbm_optimisation.builtin_periodicity) + [False] * 3)[:3]))

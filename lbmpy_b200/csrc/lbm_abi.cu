@@ -129,11 +129,20 @@ void launch_shape(const Grid& g, int zc, dim3& grid, dim3& block) {
     grid = dim3((g.nx + bx - 1) / bx, (g.ny + by - 1) / by, (g.nz + zc - 1) / zc);
 }
 
+// In-place patterns update one field (src == dst); pull and push use two.
+bool pattern_inplace(int pattern) {
+    return pattern == LBM_PATTERN_AA || pattern == LBM_PATTERN_ESOTWIST || pattern == LBM_PATTERN_ESOPULL ||
+           pattern == LBM_PATTERN_ESOPUSH;
+}
+
 int pattern_kind(const LbmPlan* p, int parity) {
     switch (p->desc.pattern) {
         case LBM_PATTERN_PULL: return PAT_PULL;
         case LBM_PATTERN_AA: return parity ? PAT_AA_ODD : PAT_AA_EVEN;
         case LBM_PATTERN_ESOTWIST: return parity ? PAT_ESO_ODD : PAT_ESO_EVEN;
+        case LBM_PATTERN_PUSH: return PAT_PUSH;
+        case LBM_PATTERN_ESOPULL: return parity ? PAT_EPULL_ODD : PAT_EPULL_EVEN;
+        case LBM_PATTERN_ESOPUSH: return parity ? PAT_EPUSH_ODD : PAT_EPUSH_EVEN;
     }
     return -1;
 }
@@ -269,6 +278,15 @@ MacroLauncher pick_get(int pat) {
         case PAT_ESO_EVEN: return &launch_get<S, R, Q, PAT_ESO_EVEN>;
         case PAT_ESO_ODD: return &launch_get<S, R, Q, PAT_ESO_ODD>;
     }
+    if constexpr (sizeof(S) >= 4) {
+        switch (pat) {
+            case PAT_PUSH: return &launch_get<S, R, Q, PAT_PUSH>;
+            case PAT_EPULL_EVEN: return &launch_get<S, R, Q, PAT_EPULL_EVEN>;
+            case PAT_EPULL_ODD: return &launch_get<S, R, Q, PAT_EPULL_ODD>;
+            case PAT_EPUSH_EVEN: return &launch_get<S, R, Q, PAT_EPUSH_EVEN>;
+            case PAT_EPUSH_ODD: return &launch_get<S, R, Q, PAT_EPUSH_ODD>;
+        }
+    }
     return nullptr;
 }
 
@@ -299,6 +317,15 @@ ReduceLauncher pick_reduce(int pat) {
         case PAT_AA_ODD: return &launch_reduce<S, Q, PAT_AA_ODD>;
         case PAT_ESO_EVEN: return &launch_reduce<S, Q, PAT_ESO_EVEN>;
         case PAT_ESO_ODD: return &launch_reduce<S, Q, PAT_ESO_ODD>;
+    }
+    if constexpr (sizeof(S) >= 4) {
+        switch (pat) {
+            case PAT_PUSH: return &launch_reduce<S, Q, PAT_PUSH>;
+            case PAT_EPULL_EVEN: return &launch_reduce<S, Q, PAT_EPULL_EVEN>;
+            case PAT_EPULL_ODD: return &launch_reduce<S, Q, PAT_EPULL_ODD>;
+            case PAT_EPUSH_EVEN: return &launch_reduce<S, Q, PAT_EPUSH_EVEN>;
+            case PAT_EPUSH_ODD: return &launch_reduce<S, Q, PAT_EPUSH_ODD>;
+        }
     }
     return nullptr;
 }
@@ -331,6 +358,15 @@ UbbLauncher pick_ubb(int pat) {
         case PAT_AA_ODD: return &launch_ubb<S, R, Q, PAT_AA_ODD>;
         case PAT_ESO_EVEN: return &launch_ubb<S, R, Q, PAT_ESO_EVEN>;
         case PAT_ESO_ODD: return &launch_ubb<S, R, Q, PAT_ESO_ODD>;
+    }
+    if constexpr (sizeof(S) >= 4) {
+        switch (pat) {
+            case PAT_PUSH: return &launch_ubb<S, R, Q, PAT_PUSH>;
+            case PAT_EPULL_EVEN: return &launch_ubb<S, R, Q, PAT_EPULL_EVEN>;
+            case PAT_EPULL_ODD: return &launch_ubb<S, R, Q, PAT_EPULL_ODD>;
+            case PAT_EPUSH_EVEN: return &launch_ubb<S, R, Q, PAT_EPUSH_EVEN>;
+            case PAT_EPUSH_ODD: return &launch_ubb<S, R, Q, PAT_EPUSH_ODD>;
+        }
     }
     return nullptr;
 }
@@ -449,7 +485,7 @@ int validate_desc(const LbmPlanDesc* d) {
     if (d->method == LBM_METHOD_CUMULANT && !d->compressible)
         return fail(LBM_E_INVALID, "Incompressible cumulant-based methods are not supported (yet).");
     if (d->store_dtype < 0 || d->store_dtype > 3) return fail(LBM_E_INVALID, "unknown dtype %d", d->store_dtype);
-    if (d->pattern < 0 || d->pattern > 2) return fail(LBM_E_INVALID, "unknown streaming pattern %d", d->pattern);
+    if (d->pattern < 0 || d->pattern > 5) return fail(LBM_E_INVALID, "unknown streaming pattern %d", d->pattern);
     if (d->force_model < 0 || d->force_model > 4) return fail(LBM_E_INVALID, "unknown force model");
     if (d->method == LBM_METHOD_CUMULANT && d->force_model != LBM_FORCE_NONE &&
         d->force_model != LBM_FORCE_CENTRAL_MOMENT)
@@ -468,7 +504,7 @@ int validate_desc(const LbmPlanDesc* d) {
                     "the learned closure is built for the D3Q27 cumulant method with orders >= 3 relaxed by 1");
     if (d->sgs == LBM_SGS_MLP && d->store_dtype != LBM_DTYPE_F32 && d->store_dtype != LBM_DTYPE_F64)
         return fail(LBM_E_UNSUPPORTED, "the learned closure is built for FP32 and FP64 storage");
-    if (d->sgs == LBM_SGS_MLP && d->pattern == LBM_PATTERN_ESOTWIST)
+    if (d->sgs == LBM_SGS_MLP && d->pattern != LBM_PATTERN_PULL && d->pattern != LBM_PATTERN_AA)
         return fail(LBM_E_UNSUPPORTED, "the learned closure is built for the pull and AA patterns");
     for (int k = 0; k < 3; ++k)
         if (d->dims[k] < 1) return fail(LBM_E_INVALID, "dims must be positive, got %d in axis %d", d->dims[k], k);
@@ -594,9 +630,9 @@ static int validate_sweep(const LbmPlan* p, const void* src, const void* dst, co
     if ((rc = check_device_ptr(p, dst, "dst", false))) return rc;
     if ((rc = check_device_ptr(p, flags, "flags", true))) return rc;
     if ((rc = check_device_ptr(p, omega_out, "omega_out", true))) return rc;
-    const bool inplace = p->desc.pattern != LBM_PATTERN_PULL;
+    const bool inplace = pattern_inplace(p->desc.pattern);
     if (inplace && src != dst) return fail(LBM_E_INVALID, "in-place streaming patterns need src == dst");
-    if (!inplace && src == dst) return fail(LBM_E_INVALID, "the pull pattern needs two distinct fields");
+    if (!inplace && src == dst) return fail(LBM_E_INVALID, "the pull and push patterns need two distinct fields");
     return LBM_OK;
 }
 
@@ -698,7 +734,7 @@ int lbm_run(const LbmPlan* p, void* a, void* b, const int64_t strides[4], const 
     if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
     if (steps < 0) return fail(LBM_E_INVALID, "steps must be >= 0");
     if (first_parity != 0 && first_parity != 1) return fail(LBM_E_INVALID, "parity must be 0 (EVEN) or 1 (ODD)");
-    const bool inplace = p->desc.pattern != LBM_PATTERN_PULL;
+    const bool inplace = pattern_inplace(p->desc.pattern);
     int rc = validate_sweep(p, a, inplace ? a : b, strides, flags, nullptr);
     if (rc) return rc;
     void* src = a;
@@ -901,7 +937,7 @@ int lbm_batch_create(const LbmPlanDesc* common, const LbmDomainDesc* domains, in
     if (t.tile_x < 1 || t.tile_y < 1 || t.tile_x * t.tile_y > 256 || t.cells_z < 1 || t.blocks_per_sm < 0)
         return fail(LBM_E_INVALID, "tiling %dx%dx%d (%d blocks/SM): need tile_x*tile_y in [1, 256], cells_z >= 1",
                     t.tile_x, t.tile_y, t.cells_z, t.blocks_per_sm);
-    if (common->pattern == LBM_PATTERN_ESOTWIST)
+    if (common->pattern != LBM_PATTERN_PULL && common->pattern != LBM_PATTERN_AA)
         return fail(LBM_E_UNSUPPORTED, "batched sweeps are built for the pull and AA patterns");
     const bool inplace = common->pattern != LBM_PATTERN_PULL;
     if (inplace && buffer_b == nullptr) buffer_b = buffer_a;

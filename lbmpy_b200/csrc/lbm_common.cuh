@@ -12,7 +12,22 @@ namespace lbm {
 enum StoreType : int { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3 };
 // SRT/TRT | raw-moment MRT | cumulant | cumulant with every order >= 3 relaxed by 1
 enum MethodKind : int { MK_POP = 0, MK_MRT = 1, MK_CUM = 2, MK_CUM1 = 3, MK_CUM1_MLP = 4 };
-enum PatternKind : int { PAT_PULL = 0, PAT_AA_EVEN = 1, PAT_AA_ODD = 2, PAT_ESO_EVEN = 3, PAT_ESO_ODD = 4 };
+enum PatternKind : int {
+    PAT_PULL = 0, PAT_AA_EVEN = 1, PAT_AA_ODD = 2, PAT_ESO_EVEN = 3, PAT_ESO_ODD = 4,
+    PAT_PUSH = 5, PAT_EPULL_EVEN = 6, PAT_EPULL_ODD = 7, PAT_EPUSH_EVEN = 8, PAT_EPUSH_ODD = 9
+};
+
+// Whether direction (x, y, z) sits at an even position of lbmpy's 'lehmann' ordering (stencils.py,
+// D3Q19 / D3Q27 'lehmann', which lists each direction right before its inverse; the rest
+// population is at position 0).  EsoPull / EsoPush (fieldaccess.py:184-318) stream the even ones
+// on one side of the collision and the odd ones on the other.
+LBM_HD constexpr bool lehmann_even(int x, int y, int z) {
+    return (x == 0 && y == 0 && z == 0) || (x == -1 && y == 0 && z == 0) || (x == 0 && y == -1 && z == 0) ||
+           (x == 0 && y == 0 && z == -1) || (x == -1 && y == -1 && z == 0) || (x == -1 && y == 0 && z == -1) ||
+           (x == 0 && y == -1 && z == -1) || (x == -1 && y == 1 && z == 0) || (x == -1 && y == 0 && z == 1) ||
+           (x == 0 && y == -1 && z == 1) || (x == -1 && y == -1 && z == -1) || (x == -1 && y == -1 && z == 1) ||
+           (x == -1 && y == 1 && z == -1) || (x == 1 && y == -1 && z == -1);
+}
 enum ForceKind : int { FM_NONE = 0, FM_GUO = 1, FM_CENTRAL = 2, FM_SIMPLE = 3, FM_LUO = 4 };
 
 // Cell flags (uint8, ghost-layered domain): low 3 bits = cell type, bit 7 = fluid cell with at

@@ -127,6 +127,15 @@ SweepLauncher pick_sweep_pattern(int pat) {
         case PAT_ESO_EVEN: return &launch_sweep<S, R, Q, MK, PAT_ESO_EVEN>;
         case PAT_ESO_ODD: return &launch_sweep<S, R, Q, MK, PAT_ESO_ODD>;
     }
+    if constexpr (sizeof(S) >= 4) {
+        switch (pat) {
+            case PAT_PUSH: return &launch_sweep<S, R, Q, MK, PAT_PUSH>;
+            case PAT_EPULL_EVEN: return &launch_sweep<S, R, Q, MK, PAT_EPULL_EVEN>;
+            case PAT_EPULL_ODD: return &launch_sweep<S, R, Q, MK, PAT_EPULL_ODD>;
+            case PAT_EPUSH_EVEN: return &launch_sweep<S, R, Q, MK, PAT_EPUSH_EVEN>;
+            case PAT_EPUSH_ODD: return &launch_sweep<S, R, Q, MK, PAT_EPUSH_ODD>;
+        }
+    }
     return nullptr;
 }
 
@@ -138,6 +147,15 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         case PAT_AA_ODD: return &launch_set_eq<S, R, Q, MK, PAT_AA_ODD>;
         case PAT_ESO_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_ESO_EVEN>;
         case PAT_ESO_ODD: return &launch_set_eq<S, R, Q, MK, PAT_ESO_ODD>;
+    }
+    if constexpr (sizeof(S) >= 4) {
+        switch (pat) {
+            case PAT_PUSH: return &launch_set_eq<S, R, Q, MK, PAT_PUSH>;
+            case PAT_EPULL_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_EPULL_EVEN>;
+            case PAT_EPULL_ODD: return &launch_set_eq<S, R, Q, MK, PAT_EPULL_ODD>;
+            case PAT_EPUSH_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_EPUSH_EVEN>;
+            case PAT_EPUSH_ODD: return &launch_set_eq<S, R, Q, MK, PAT_EPUSH_ODD>;
+        }
     }
     return nullptr;
 }

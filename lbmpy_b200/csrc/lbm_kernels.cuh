@@ -6,6 +6,9 @@
 //   AA even   read f[x](i)                    write f[x](inv i)
 //   AA odd    read f[x - c_i](inv i)          write f[x + c_i](i)
 //   EsoTwist  even/odd with offsets max(-c,0) / max(c,0) (fieldaccess.py:160-181)
+//   push      read src[x](i)                  write dst[x + c_i](i)   (fieldaccess.py:78-87)
+//   EsoPull / EsoPush  in place, by the direction's parity in the 'lehmann' ordering
+//                                                                     (fieldaccess.py:184-318)
 // Periodicity is an index wrap instead of ghost-layer copies, and NoSlip / UBB bounce-back
 // (boundaries/boundaryconditions.py:128-139, 794-841) is fused into the read: where lbmpy's
 // boundary kernel would have written the wall slot, the sweep reads the value that kernel
@@ -16,29 +19,39 @@
 namespace lbm {
 
 template <int PAT> struct Access {
+    template <int Q>
+    LBM_HD static constexpr bool leven(int i) { return lehmann_even(Lat<Q>::cx(i), Lat<Q>::cy(i), Lat<Q>::cz(i)); }
     // read location of direction i: offset (ox, oy, oz) and slot
     template <int Q>
     LBM_HD static constexpr int rslot(int i) {
-        return (PAT == PAT_AA_ODD || PAT == PAT_ESO_ODD) ? Lat<Q>::inv(i) : i;
+        return (PAT == PAT_AA_ODD || PAT == PAT_ESO_ODD || PAT == PAT_EPULL_ODD || PAT == PAT_EPUSH_EVEN)
+                   ? Lat<Q>::inv(i) : i;
     }
     template <int Q>
     LBM_HD static constexpr int roff(int i, int d) {
         const int c = d == 0 ? Lat<Q>::cx(i) : (d == 1 ? Lat<Q>::cy(i) : Lat<Q>::cz(i));
         return PAT == PAT_PULL ? -c
+             : PAT == PAT_PUSH ? 0
              : PAT == PAT_AA_EVEN ? 0
              : PAT == PAT_AA_ODD ? -c
+             : (PAT == PAT_EPULL_EVEN || PAT == PAT_EPULL_ODD) ? (leven<Q>(i) ? -c : 0)
+             : (PAT == PAT_EPUSH_EVEN || PAT == PAT_EPUSH_ODD) ? (leven<Q>(i) ? 0 : -c)
              : (c < 0 ? -c : 0);   // EsoTwist: max(-c, 0)
     }
     template <int Q>
     LBM_HD static constexpr int wslot(int i) {
-        return (PAT == PAT_AA_EVEN || PAT == PAT_ESO_EVEN) ? Lat<Q>::inv(i) : i;
+        return (PAT == PAT_AA_EVEN || PAT == PAT_ESO_EVEN || PAT == PAT_EPULL_EVEN || PAT == PAT_EPUSH_ODD)
+                   ? Lat<Q>::inv(i) : i;
     }
     template <int Q>
     LBM_HD static constexpr int woff(int i, int d) {
         const int c = d == 0 ? Lat<Q>::cx(i) : (d == 1 ? Lat<Q>::cy(i) : Lat<Q>::cz(i));
         return PAT == PAT_PULL ? 0
+             : PAT == PAT_PUSH ? c
              : PAT == PAT_AA_EVEN ? 0
              : PAT == PAT_AA_ODD ? c
+             : (PAT == PAT_EPULL_EVEN || PAT == PAT_EPULL_ODD) ? (leven<Q>(i) ? 0 : c)
+             : (PAT == PAT_EPUSH_EVEN || PAT == PAT_EPUSH_ODD) ? (leven<Q>(i) ? c : 0)
              : (c > 0 ? c : 0);    // EsoTwist: max(c, 0)
     }
 };
@@ -49,7 +62,11 @@ template <int PAT> struct PrevPattern {
                                : PAT == PAT_AA_ODD ? PAT_AA_EVEN
                                : PAT == PAT_ESO_EVEN ? PAT_ESO_ODD
                                : PAT == PAT_ESO_ODD ? PAT_ESO_EVEN
-                               : PAT_PULL;
+                               : PAT == PAT_EPULL_EVEN ? PAT_EPULL_ODD
+                               : PAT == PAT_EPULL_ODD ? PAT_EPULL_EVEN
+                               : PAT == PAT_EPUSH_EVEN ? PAT_EPUSH_ODD
+                               : PAT == PAT_EPUSH_ODD ? PAT_EPUSH_EVEN
+                               : PAT;
 };
 
 // Eddy viscosity of the learned closure for the sweep with MK_CUM1_MLP; defined (with the

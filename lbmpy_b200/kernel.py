@@ -21,7 +21,8 @@ from .fields import check_pdf_tensor
 from . import forcemodels
 
 _METHOD = {"srt": N.METHOD_SRT, "trt": N.METHOD_TRT, "mrt": N.METHOD_MRT, "cumulant": N.METHOD_CUMULANT}
-_PATTERN = {"pull": N.PATTERN_PULL, "aa": N.PATTERN_AA, "esotwist": N.PATTERN_ESOTWIST}
+_PATTERN = {"pull": N.PATTERN_PULL, "aa": N.PATTERN_AA, "esotwist": N.PATTERN_ESOTWIST, "push": N.PATTERN_PUSH,
+            "esopull": N.PATTERN_ESOPULL, "esopush": N.PATTERN_ESOPUSH}
 _DT = {"float64": N.DTYPE_F64, "float32": N.DTYPE_F32, "float16": N.DTYPE_F16, "bfloat16": N.DTYPE_BF16}
 
 

@@ -6,8 +6,9 @@ lbmpy's sync -> boundary -> sweep -> swap sequence (:271-282) becomes sweep -> s
 lbmpy, the velocity and density arrays the user sees are host (numpy) arrays that ``run`` fills
 at the end (post_run, :311-314) and that ``set_pdf_fields_from_macroscopic_values`` reads.
 
-Extension over lbmpy: ``streaming_pattern='aa'`` / ``'esotwist'`` run in place on one field
-(lbmpy's step supports two-field patterns only, :153-156 and :282).
+Extension over lbmpy: ``streaming_pattern='aa'`` / ``'esotwist'`` / ``'esopull'`` / ``'esopush'``
+run in place on one field (lbmpy's step supports two-field patterns only, :153-156 and :282);
+``'push'`` runs on two fields like ``'pull'``.
 """
 from __future__ import annotations
 

@@ -17,7 +17,7 @@ from . import _native as N
 from .enums import Target, Timestep
 from .fields import check_pdf_tensor, dtype_name
 
-_PATTERNS = ("pull", "aa", "esotwist")
+_PATTERNS = ("pull", "push", "aa", "esotwist", "esopull", "esopush")
 
 
 def _rule_for(lb_method, streaming_pattern, storage_dtype, collision_rule=None):

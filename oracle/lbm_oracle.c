@@ -63,13 +63,28 @@ typedef struct {
     int64_t s[4];             /* element strides of x, y, z, q */
 } om_grid;
 
-enum { P_PULL = 0, P_PUSH = 1, P_AA = 2, P_ESOTWIST = 3 };
+enum { P_PULL = 0, P_PUSH = 1, P_AA = 2, P_ESOTWIST = 3, P_ESOPULL = 4, P_ESOPUSH = 5 };
+
+/* Whether direction c sits at an even position of lbmpy's 'lehmann' ordering (stencils.py,
+ * D2Q9 / D3Q19 / D3Q27 'lehmann'; used by fieldaccess.py:184-318 through _get_lehmann_stencil,
+ * :371-388).  That ordering lists each direction right before its inverse, so the even ones are
+ * the second of each pair; the rest population is at position 0. */
+static int lehmann_even(const int c[3]) {
+    static const int even[13][3] = {{-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {-1, -1, 0}, {-1, 0, -1},
+                                    {0, -1, -1}, {-1, 1, 0}, {-1, 0, 1}, {0, -1, 1}, {-1, -1, -1},
+                                    {-1, -1, 1}, {-1, 1, -1}, {1, -1, -1}};
+    int k;
+    if (c[0] == 0 && c[1] == 0 && c[2] == 0) return 1;
+    for (k = 0; k < 13; ++k)
+        if (c[0] == even[k][0] && c[1] == even[k][1] && c[2] == even[k][2]) return 1;
+    return 0;
+}
 
 /* ------------------------------------------------------------------------------------------ */
 static double ipow(double b, int e) { double r = 1.0; while (e-- > 0) r *= b; return r; }
 
 /* Accessor table: offset and slot of the read (rw=0) or write (rw=1) of direction i.
- * fieldaccess.py:66-181.  parity 0 = EVEN, 1 = ODD (two-field patterns ignore it). */
+ * fieldaccess.py:66-318.  parity 0 = EVEN, 1 = ODD (two-field patterns ignore it). */
 static void accessor(const om_method* m, int pattern, int parity, int rw, int i, int off[3], int* slot) {
     const int* c = m->c[i];
     int d;
@@ -92,6 +107,20 @@ static void accessor(const om_method* m, int pattern, int parity, int rw, int i,
         if (parity == 0) *slot = rw == 0 ? i : m->inv[i];
         else *slot = rw == 0 ? m->inv[i] : i;
         return;
+    case P_ESOPULL: {     /* fieldaccess.py:184-232: even-position directions stream on read */
+        const int e = lehmann_even(c);
+        for (d = 0; d < 3; ++d) off[d] = rw == 0 ? (e ? -c[d] : 0) : (e ? 0 : c[d]);
+        if (parity == 0) *slot = rw == 0 ? i : m->inv[i];
+        else *slot = rw == 0 ? m->inv[i] : i;
+        return;
+    }
+    case P_ESOPUSH: {     /* fieldaccess.py:235-318: odd-position directions stream on read */
+        const int e = lehmann_even(c);
+        for (d = 0; d < 3; ++d) off[d] = rw == 0 ? (e ? 0 : -c[d]) : (e ? c[d] : 0);
+        if (parity == 0) *slot = rw == 0 ? m->inv[i] : i;
+        else *slot = rw == 0 ? i : m->inv[i];
+        return;
+    }
     }
 }
 
@@ -671,7 +700,8 @@ void om_get_macroscopic(const om_method* m, const om_grid* gr, int pattern, int 
  * result ends up in b. */
 int om_run(const om_method* m, const om_grid* gr, int pattern, int* parity, int steps,
            const int periodic[3], const uint8_t* flags, const double ubb_u[3], double* a, double* b) {
-    int t, inplace = (pattern == P_AA || pattern == P_ESOTWIST), swapped = 0;
+    int t, inplace = (pattern == P_AA || pattern == P_ESOTWIST || pattern == P_ESOPULL || pattern == P_ESOPUSH),
+        swapped = 0;
     double *src = a, *dst = b;
     for (t = 0; t < steps; ++t) {
         om_periodic_sync(m, gr, pattern, *parity, periodic, src);
@@ -704,3 +734,10 @@ void om_reduce(const om_method* m, const om_grid* gr, int pattern, int prev_pari
 }
 
 int om_sizeof_method(void) { return (int)sizeof(om_method); }
+
+/* The accessor table of one pattern / parity: read (rw = 0) or write (rw = 1) offset off[3*i..]
+ * and slot slot[i] of every direction i. */
+void om_accessor_table(const om_method* m, int pattern, int parity, int rw, int* off, int* slot) {
+    int i;
+    for (i = 0; i < m->Q; ++i) accessor(m, pattern, parity, rw, i, off + 3 * i, slot + i);
+}

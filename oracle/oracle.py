@@ -22,7 +22,7 @@ _LIB = None
 
 QMAX, TMAX = 27, 40
 MLP_NPARAM = 10 * 32 + 32 + 32 * 32 + 32 + 32 + 1 + 1
-PATTERNS = {"pull": 0, "push": 1, "aa": 2, "esotwist": 3}
+PATTERNS = {"pull": 0, "push": 1, "aa": 2, "esotwist": 3, "esopull": 4, "esopush": 5}
 
 
 class OmMethod(ctypes.Structure):
@@ -248,6 +248,16 @@ class Oracle:
         per = (ctypes.c_int * 3)(*[int(p) for p in periodic])
         lib().om_periodic_sync(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], prev_parity, per,
                                self._ptr(f))
+
+    def accessor_table(self, pattern, parity, rw):
+        """Offsets [Q, 3] and slots [Q] where direction i is read (rw = 0) or written (rw = 1)."""
+        q = self._m.Q
+        off = np.zeros((q, 3), np.int32)
+        slot = np.zeros(q, np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        lib().om_accessor_table(ctypes.byref(self._m), PATTERNS[pattern], parity, rw, off.ctypes.data_as(ip),
+                                slot.ctypes.data_as(ip))
+        return off, slot
 
     def reduce(self, f, pattern="pull", prev_parity=0, flags=None):
         g = self._grid(f)

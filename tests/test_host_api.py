@@ -141,7 +141,9 @@ def test_unsupported_configurations_fail_loudly():
         L.create_lb_method(L.LBMConfig(stencil=L.Stencil.D2Q9, relaxation_rate=1.0))
     with pytest.raises(NotImplementedError):
         L.create_lb_function(lbm_config=L.LBMConfig(stencil=L.Stencil.D3Q19, relaxation_rate=1.0,
-                                                    streaming_pattern="push"))
+                                                    streaming_pattern="esopull", timestep=L.Timestep.EVEN),
+                             lbm_optimisation=L.LBMOptimisation(storage_dtype="float16"),
+                             config=L.CreateKernelConfig(data_type="float32"))
     with pytest.raises(NotImplementedError):
         L.create_lb_method(L.LBMConfig(stencil=L.Stencil.D3Q19, method=L.Method.CENTRAL_MOMENT, relaxation_rate=1))
     with pytest.raises(ValueError):
