@@ -16,7 +16,8 @@
  * must be 1 and sy, sz, sq are passed in `strides` = {1, sy, sz, sq}.
  *
  * Flag field (optional): uint8 over the ghost-inclusive domain, x fastest, contiguous:
- * index x + (nx+2)*(y + (ny+2)*z).  Low 3 bits: 0 fluid, 1 NoSlip, 2..5 UBB number 0..3;
+ * index x + (nx+2)*(y + (ny+2)*z).  Low 3 bits: 0 fluid, 1 NoSlip, 2..5 UBB number 0..3,
+ * 6 FixedDensity (density `fixed_density` of the plan);
  * bit 7 marks fluid cells with a boundary neighbour (lbm_flags_finalize sets it).
  */
 #ifndef LBM_B200_H
@@ -69,6 +70,8 @@ typedef struct LbmPlanDesc {
     double ubb_velocity[4][3];  /* wall velocity of UBB numbers 0..3 */
     int32_t dims[3];            /* interior cells nx, ny, nz */
     int32_t periodic[3];
+    double fixed_density;       /* wall density of FixedDensity cells (flag type 6); 0: none
+                                   (boundaries/boundaryconditions.py:1044-1099) */
 } LbmPlanDesc;
 
 typedef struct LbmPlan LbmPlan;

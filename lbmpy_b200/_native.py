@@ -47,6 +47,7 @@ class LbmPlanDesc(ctypes.Structure):
         ("ubb_velocity", (ctypes.c_double * 3) * 4),
         ("dims", ctypes.c_int32 * 3),
         ("periodic", ctypes.c_int32 * 3),
+        ("fixed_density", ctypes.c_double),
     ]
 
 

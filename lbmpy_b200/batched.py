@@ -201,6 +201,8 @@ class LatticeBoltzmannBatch:
                 flag_offsets.append(-1)
         common = None
         for k, size in enumerate(self.domain_sizes):
+            if self._handlings[k].fixed_density is not None:
+                raise NotImplementedError("FixedDensity boundaries are not built for batches")
             d = build_desc(self.update_rule, size, self.periodicity[k], self.kernel_params[k],
                            self._handlings[k].ubb_velocities)
             if common is None:

@@ -16,7 +16,7 @@ import torch
 
 from . import _native as N
 
-FLUID, NOSLIP, UBB0 = 0, 1, 2
+FLUID, NOSLIP, UBB0, FIXED_DENSITY = 0, 1, 2, 6
 MAX_UBB = 4
 
 
@@ -64,6 +64,21 @@ class UBB(LbBoundary):
         return self._velocity
 
 
+class FixedDensity(LbBoundary):
+    """Prescribed density (pressure p = rho / 3) at the wall (boundaryconditions.py:1044-1099):
+    f_in(inv i) = 2 feq_even_i(rho_w, u) - f*_i, with feq_even the part of the method's equilibrium
+    that is even in u and u the fluid cell's velocity from its outgoing populations at density
+    rho_w.  One density per domain; force-free methods."""
+
+    def __init__(self, density, name=None):
+        if callable(density):
+            raise NotImplementedError("density callbacks are not built; use a constant density")
+        self.density = float(density)
+        if not self.density > 0:
+            raise ValueError("FixedDensity needs a positive density")
+        super().__init__(name)
+
+
 def slice_from_direction(direction_name: str, dim: int, normal_offset=0, tangential_offset=0):
     """pystencils' compass-direction slices over the ghost-inclusive array: 'N' is the last y
     layer (the ghost layer), 'S' the first, 'E'/'W' in x, 'T'/'B' in z."""
@@ -93,6 +108,7 @@ class LatticeBoltzmannBoundaryHandling:
         ex, ey, ez = (s + 2 for s in self.shape)
         self._host = np.zeros((ez, ey, ex), dtype=np.uint8)   # [z, y, x]
         self._ubbs: List[UBB] = []
+        self._fixed_density: Optional[float] = None
         self._dev: Optional[torch.Tensor] = None
         self._finalized_for = None
 
@@ -110,7 +126,13 @@ class LatticeBoltzmannBoundaryHandling:
                 raise ValueError(f"at most {MAX_UBB} different UBB velocities are supported")
             self._ubbs.append(boundary_obj)
             return UBB0 + len(self._ubbs) - 1
-        raise NotImplementedError(f"boundary {type(boundary_obj).__name__} is not built (NoSlip and UBB are)")
+        if isinstance(boundary_obj, FixedDensity):
+            if self._fixed_density is not None and self._fixed_density != boundary_obj.density:
+                raise ValueError("one FixedDensity density per domain is supported")
+            self._fixed_density = boundary_obj.density
+            return FIXED_DENSITY
+        raise NotImplementedError(f"boundary {type(boundary_obj).__name__} is not built (NoSlip, UBB and "
+                                  "FixedDensity are)")
 
     def set_boundary(self, boundary_obj, slice_obj=None, mask_callback=None, ghost_layers=True,
                      inner_ghost_layers=True, replace=True, force_flag_value=None):
@@ -150,6 +172,11 @@ class LatticeBoltzmannBoundaryHandling:
     @property
     def ubb_velocities(self):
         return [u.velocity for u in self._ubbs]
+
+    @property
+    def fixed_density(self):
+        """Density of the FixedDensity cells, if any are set."""
+        return self._fixed_density if bool(((self._host & 7) == FIXED_DENSITY).any()) else None
 
     @property
     def has_boundaries(self) -> bool:

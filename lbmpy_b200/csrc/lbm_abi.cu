@@ -224,6 +224,16 @@ bool pair_applicable(const LbmPlan* p, const void* src, const void* dst, const i
     return pair_launcher(p, pat) != nullptr;
 }
 
+SweepLauncher fixed_density_launcher(const LbmPlan* p, int pat) {
+    if (p->q == 19 && p->mk == MK_POP) return fixed_density_q19_pop(p->store, pat);
+    if (p->q == 19 && p->mk == MK_MRT) return fixed_density_q19_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_POP) return fixed_density_q27_pop(p->store, pat);
+    if (p->q == 27 && p->mk == MK_MRT) return fixed_density_q27_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM) return fixed_density_q27_cum(p->store, pat);
+    if (p->q == 27 && (p->mk == MK_CUM1 || p->mk == MK_CUM1_MLP)) return fixed_density_q27_cum1(p->store, pat);
+    return nullptr;
+}
+
 StagedLauncher staged_launcher(const LbmPlan* p, int pat) {
     if (p->q == 19 && p->mk == MK_POP) return sweep_staged_q19_pop(p->store, pat);
     if (p->q == 19 && p->mk == MK_MRT) return sweep_staged_q19_mrt(p->store, pat);
@@ -457,6 +467,7 @@ int fill_physics(LbmPlan* p, const LbmPlanDesc* d) {
     for (int u = 0; u < MAX_UBB; ++u)
         for (int k = 0; k < 3; ++k) ph.ubb[u][k] = d->ubb_velocity[u][k];
     if (d->method == LBM_METHOD_SRT) ph.rates[1] = ph.rates[0];
+    ph.fixed_density = d->fixed_density;
     return LBM_OK;
 }
 
@@ -506,6 +517,9 @@ int validate_desc(const LbmPlanDesc* d) {
         return fail(LBM_E_UNSUPPORTED, "the learned closure is built for FP32 and FP64 storage");
     if (d->sgs == LBM_SGS_MLP && d->pattern != LBM_PATTERN_PULL && d->pattern != LBM_PATTERN_AA)
         return fail(LBM_E_UNSUPPORTED, "the learned closure is built for the pull and AA patterns");
+    if (!(d->fixed_density >= 0.0)) return fail(LBM_E_INVALID, "fixed_density must be >= 0 (0: no FixedDensity cells)");
+    if (d->fixed_density > 0.0 && d->force_model != LBM_FORCE_NONE)
+        return fail(LBM_E_UNSUPPORTED, "FixedDensity boundaries are built for force-free methods");
     for (int k = 0; k < 3; ++k)
         if (d->dims[k] < 1) return fail(LBM_E_INVALID, "dims must be positive, got %d in axis %d", d->dims[k], k);
     if (d->dims[1] > 65535 * 8 || d->dims[2] > 65535)
@@ -668,6 +682,14 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
         cudaError_t e = U(a, p->ubb_rho, ug, ub, stream);
         if (e != cudaSuccess) return cuda_fail(e, "wall-density launch");
         a.ubb_rho = p->ubb_rho;
+    }
+    if (flags != nullptr && p->desc.fixed_density > 0) {
+        SweepLauncher F = fixed_density_launcher(p, pat);
+        if (F == nullptr) return fail(LBM_E_UNSUPPORTED, "no FixedDensity kernel for this storage type / pattern");
+        dim3 fg, fb;
+        launch_shape(a.g, 1, fg, fb);
+        cudaError_t e = F(a, fg, fb, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "FixedDensity launch");
     }
     const int variant = sweep_variant(p, src, dst, strides, pat, omega_out);
     if (variant == LBM_VARIANT_STAGED) {
@@ -939,6 +961,8 @@ int lbm_batch_create(const LbmPlanDesc* common, const LbmDomainDesc* domains, in
                     t.tile_x, t.tile_y, t.cells_z, t.blocks_per_sm);
     if (common->pattern != LBM_PATTERN_PULL && common->pattern != LBM_PATTERN_AA)
         return fail(LBM_E_UNSUPPORTED, "batched sweeps are built for the pull and AA patterns");
+    if (common->fixed_density != 0.0)
+        return fail(LBM_E_UNSUPPORTED, "batched sweeps are built without FixedDensity boundaries");
     const bool inplace = common->pattern != LBM_PATTERN_PULL;
     if (inplace && buffer_b == nullptr) buffer_b = buffer_a;
     if (inplace && buffer_b != buffer_a) return fail(LBM_E_INVALID, "in-place patterns use buffer_a only");

@@ -31,11 +31,13 @@ LBM_HD constexpr bool lehmann_even(int x, int y, int z) {
 enum ForceKind : int { FM_NONE = 0, FM_GUO = 1, FM_CENTRAL = 2, FM_SIMPLE = 3, FM_LUO = 4 };
 
 // Cell flags (uint8, ghost-layered domain): low 3 bits = cell type, bit 7 = fluid cell with at
-// least one boundary neighbour.  Type 0 fluid, 1 NoSlip, 2..5 UBB number (type - 2).
+// least one boundary neighbour.  Type 0 fluid, 1 NoSlip, 2..5 UBB number (type - 2),
+// 6 FixedDensity.
 constexpr int FLAG_TYPE_MASK = 7;
 constexpr int FLAG_NEAR_WALL = 128;
 constexpr int FLAG_NOSLIP = 1;
 constexpr int FLAG_UBB0 = 2;
+constexpr int FLAG_FIXED_DENSITY = 6;
 constexpr int MAX_UBB = 4;
 
 template <int Q> struct Lat;
@@ -112,6 +114,7 @@ struct Physics {
     uint32_t sgs_mask;     // moments (or TRT parts) whose rate is the shear rate
     int galilean;
     double ubb[MAX_UBB][3];
+    double fixed_density;  // wall density of FixedDensity cells (0: none)
 };
 
 struct Grid {

@@ -139,6 +139,33 @@ SweepLauncher pick_sweep_pattern(int pat) {
     return nullptr;
 }
 
+template <class S, class R, int Q, int MK, int PAT>
+cudaError_t launch_fixed_density(const SweepArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
+    k_fixed_density<S, R, Q, MK, PAT><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S, class R, int Q, int MK>
+SweepLauncher pick_fixed_density_pattern(int pat) {
+    switch (pat) {
+        case PAT_PULL: return &launch_fixed_density<S, R, Q, MK, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_fixed_density<S, R, Q, MK, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_fixed_density<S, R, Q, MK, PAT_AA_ODD>;
+        case PAT_ESO_EVEN: return &launch_fixed_density<S, R, Q, MK, PAT_ESO_EVEN>;
+        case PAT_ESO_ODD: return &launch_fixed_density<S, R, Q, MK, PAT_ESO_ODD>;
+    }
+    if constexpr (sizeof(S) >= 4) {
+        switch (pat) {
+            case PAT_PUSH: return &launch_fixed_density<S, R, Q, MK, PAT_PUSH>;
+            case PAT_EPULL_EVEN: return &launch_fixed_density<S, R, Q, MK, PAT_EPULL_EVEN>;
+            case PAT_EPULL_ODD: return &launch_fixed_density<S, R, Q, MK, PAT_EPULL_ODD>;
+            case PAT_EPUSH_EVEN: return &launch_fixed_density<S, R, Q, MK, PAT_EPUSH_EVEN>;
+            case PAT_EPUSH_ODD: return &launch_fixed_density<S, R, Q, MK, PAT_EPUSH_ODD>;
+        }
+    }
+    return nullptr;
+}
+
 template <class S, class R, int Q, int MK>
 MacroLauncher pick_set_eq_pattern(int pat) {
     switch (pat) {
@@ -194,6 +221,15 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         }                                                                                       \
         return nullptr;                                                                         \
     }                                                                                           \
+    SweepLauncher fixed_density_##NAME(int store, int pat) {                                    \
+        switch (store) {                                                                        \
+            case ST_F64: return pick_fixed_density_pattern<double, double, Q, MK>(pat);          \
+            case ST_F32: return pick_fixed_density_pattern<float, float, Q, MK>(pat);            \
+            case ST_F16: return pick_fixed_density_pattern<__half, float, Q, MK>(pat);           \
+            case ST_BF16: return pick_fixed_density_pattern<__nv_bfloat16, float, Q, MK>(pat);  \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }                                                                                           \
     SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
         switch (store) {                                                                        \
             case ST_F32: return pick_pair_pattern<float, Q, MK>(pat);                            \
@@ -238,6 +274,12 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         return nullptr;                                                                         \
     }                                                                                           \
     SweepLauncher sweep_quad_##NAME(int, int) { return nullptr; }                               \
+    SweepLauncher fixed_density_##NAME(int store, int pat) {                                    \
+        if (pat != PAT_PULL && pat != PAT_AA_EVEN && pat != PAT_AA_ODD) return nullptr;          \
+        if (store == ST_F64) return pick_fixed_density_pattern<double, double, Q, MK>(pat);     \
+        if (store == ST_F32) return pick_fixed_density_pattern<float, float, Q, MK>(pat);       \
+        return nullptr;                                                                         \
+    }                                                                                           \
     StagedLauncher sweep_staged_##NAME(int store, int pat) {                                    \
         if (store == ST_F64) return pick_staged_pattern<double, double, Q, MK>(pat);            \
         if (store == ST_F32) return pick_staged_pattern<float, float, Q, MK>(pat);              \
@@ -264,6 +306,7 @@ MacroLauncher pick_set_eq_pattern(int pat) {
     SweepLauncher sweep_pair_##NAME(int store, int pat); \
     SweepLauncher sweep_quad_##NAME(int store, int pat); \
     StagedLauncher sweep_staged_##NAME(int store, int pat); \
+    SweepLauncher fixed_density_##NAME(int store, int pat); \
     MacroLauncher set_eq_##NAME(int store, int pat);
 
 LBM_DECLARE_FAMILY(q19_pop)

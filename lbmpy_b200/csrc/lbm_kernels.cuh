@@ -105,7 +105,7 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
 #pragma unroll
     for (int i = 1; i < Q; ++i) {
         const int bt = g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK;
-        if (bt == 0) continue;
+        if (bt == 0 || bt == FLAG_FIXED_DENSITY) continue;   // FixedDensity: written by k_fixed_density
         // f_out(x, inv i): where the previous step wrote direction inv(i) of this cell
         const int j = L::inv(i);
         const int off = nb.off(PA::template woff<Q>(j, 0), PA::template woff<Q>(j, 1), PA::template woff<Q>(j, 2));
@@ -319,6 +319,67 @@ __global__ void __launch_bounds__(256) k_set_equilibrium(const MacroArgs a) {
     for (int i = 0; i < Q; ++i) {
         const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
         Conv<S, R>::st(dst + eidx(A::template wslot<Q>(i) * g.sq, cell + off), f[i]);
+    }
+}
+
+// FixedDensity links (boundaries/boundaryconditions.py:1044-1099), before the sweep as lbmpy's
+// boundary kernel runs before its sweep.  For a fluid cell x whose neighbour x - c_i is a
+// FixedDensity cell, the population the sweep reads in direction i becomes
+//   2 feq_even_i(rho_w, u) - f*_{inv i}(x),   feq_even_i = (feq_i + feq_{inv i}) / 2,
+// the part of the method's equilibrium that is even in u, with u from x's outgoing populations of
+// the previous step at density rho_w (j / rho_w compressible, j otherwise).  It is stored where
+// the sweep reads it: a slot that only the boundary cell's own update would write, so no fluid
+// cell's outgoing value is overwritten, in place or not.  Force-free methods (host-checked).
+template <class S, class R, int Q, int MK, int PAT>
+__global__ void __launch_bounds__(256) k_fixed_density(const SweepArgs a) {
+    using L = Lat<Q>;
+    using A = Access<PAT>;
+    using PA = Access<PrevPattern<PAT>::value>;
+    constexpr int EQ = (MK == MK_CUM1 || MK == MK_CUM1_MLP) ? MK_CUM : MK;
+    const Grid& g = a.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.nx || y >= g.ny || !row_flagged(g, y, z)) return;
+    const int fcell = (x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz;
+    const int fl = g.flags[fcell];
+    if ((fl & FLAG_TYPE_MASK) || !(fl & FLAG_NEAR_WALL)) return;
+    NbrOffsets fo;
+    {
+        Grid gf = g;
+        gf.sy = g.fsy;
+        gf.sz = g.fsz;
+        fo.init(gf, x, y, z);
+    }
+    bool any = false;
+#pragma unroll
+    for (int i = 1; i < Q; ++i)
+        if ((g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK) == FLAG_FIXED_DENSITY) any = true;
+    if (!any) return;
+    NbrOffsets nb;
+    nb.init(g, x, y, z);
+    const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
+    S* f = const_cast<S*>(static_cast<const S*>(a.src));
+    R out[Q];
+    R jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const int off = nb.off(PA::template woff<Q>(k, 0), PA::template woff<Q>(k, 1), PA::template woff<Q>(k, 2));
+        out[k] = Conv<S, R>::ld(f + eidx(PA::template wslot<Q>(k) * g.sq, cell + off));
+        jx += R(L::cx(k)) * out[k];
+        jy += R(L::cy(k)) * out[k];
+        jz += R(L::cz(k)) * out[k];
+    }
+    const R rw = R(a.p.fixed_density);
+    const R s = a.p.compressible ? R(1) / rw : R(1);
+    R feq[Q];
+    equilibrium<Q, R, EQ>(feq, rw, jx * s, jy * s, jz * s, a.p);
+#pragma unroll
+    for (int i = 1; i < Q; ++i) {
+        if ((g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK) != FLAG_FIXED_DENSITY) continue;
+        const int q = L::inv(i);
+        const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
+        Conv<S, R>::st(f + eidx(A::template rslot<Q>(i) * g.sq, cell + off), feq[q] + feq[i] - out[q]);
     }
 }
 

@@ -16,7 +16,7 @@ from typing import Dict, Optional, Sequence
 import torch
 
 from . import _native as N
-from .enums import Timestep
+from .enums import Timestep, is_inplace
 from .fields import check_pdf_tensor
 from . import forcemodels
 
@@ -58,7 +58,7 @@ def free_parameters(update_rule) -> set:
 
 
 def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None,
-               rates_needed: bool = True) -> N.LbmPlanDesc:
+               rates_needed: bool = True, fixed_density=None) -> N.LbmPlanDesc:
     """Resolves an update rule plus parameter values into the C plan descriptor.  Plans that only
     run the getter / setter do not need relaxation rates (rates_needed=False)."""
     rule = update_rule.collision_rule
@@ -107,6 +107,7 @@ def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None,
         vel = list(vel) + [0.0] * 3
         for k in range(3):
             d.ubb_velocity[u][k] = float(vel[k])
+    d.fixed_density = float(fixed_density) if fixed_density is not None else 0.0
     for k in range(3):
         d.dims[k] = int(dims[k])
         d.periodic[k] = int(bool(periodic[k]))
@@ -167,8 +168,9 @@ class LbKernel:
     def q(self):
         return self.method.stencil.Q
 
-    def plan(self, dims, periodic, params=None, ubb_velocities=None) -> N.Plan:
-        desc = build_desc(self.update_rule, dims, periodic, params or {}, ubb_velocities)
+    def plan(self, dims, periodic, params=None, ubb_velocities=None, fixed_density=None) -> N.Plan:
+        desc = build_desc(self.update_rule, dims, periodic, params or {}, ubb_velocities,
+                          fixed_density=fixed_density)
         closure = self.update_rule.collision_rule.closure
         if closure is not None:
             closure.ensure_uploaded()
@@ -190,10 +192,10 @@ class LbKernel:
         return v
 
     def bind(self, pdfs: torch.Tensor, periodic, flags=None, ubb_velocities=None, params=None,
-             stream=None) -> BoundSweep:
+             stream=None, fixed_density=None) -> BoundSweep:
         check_pdf_tensor(pdfs, self.q, self.update_rule.storage_dtype, "pdfs")
         dims = [s - 2 for s in pdfs.shape[:3]]
-        plan = self.plan(dims, periodic, params or {}, ubb_velocities)
+        plan = self.plan(dims, periodic, params or {}, ubb_velocities, fixed_density)
         return BoundSweep(plan, pdfs.stride(), flags, _stream_handle(stream))
 
     def _parity(self):
@@ -207,7 +209,7 @@ class LbKernel:
             src = kwargs.pop("pdfs", None)
         if src is None:
             raise ValueError(f"missing PDF field {ur.field_name!r}")
-        inplace = ur.streaming_pattern != "pull"
+        inplace = is_inplace(ur.streaming_pattern)
         dst = kwargs.pop(ur.temporary_field_name, None)
         if inplace:
             dst = src
@@ -215,6 +217,7 @@ class LbKernel:
             raise ValueError(f"missing temporary PDF field {ur.temporary_field_name!r} for the pull pattern")
         flags = kwargs.pop("flags", None)
         ubb = kwargs.pop("ubb_velocities", None)
+        fixed_density = kwargs.pop("fixed_density", None)
         periodic = kwargs.pop("periodicity", ur.builtin_periodicity)
         omega_out = kwargs.pop("omega_out", None)
         stream = kwargs.pop("stream", None)
@@ -235,7 +238,7 @@ class LbKernel:
         if omega_out is not None:
             if omega_out.dtype != torch.float32 or omega_out.numel() != dims[0] * dims[1] * dims[2]:
                 raise ValueError("omega_out must be a float32 tensor with one entry per interior cell")
-        plan = self.plan(dims, periodic, kwargs, ubb)
+        plan = self.plan(dims, periodic, kwargs, ubb, fixed_density)
         strides = N.i64_array(src.stride())
         par = self._parity() if parity is None else int(parity)
         N.check(N.lib().lbm_sweep(plan.handle, ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr()),

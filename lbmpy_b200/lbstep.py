@@ -201,7 +201,7 @@ class LatticeBoltzmannStep:
         if not self._boundary_handling.has_boundaries:
             return None
         plan = kernel.plan([d for d in self._domain], self.periodicity, self.kernel_params,
-                           self._boundary_handling.ubb_velocities)
+                           self._boundary_handling.ubb_velocities, self._boundary_handling.fixed_density)
         return self._boundary_handling.flags(plan)
 
     def _bound(self):
@@ -213,7 +213,8 @@ class LatticeBoltzmannStep:
         if getattr(self, "_bound_key", None) != key or self._bound_sweep is None:
             k = self._kernels[0]
             flags = self._flags(k)
-            self._bound_sweep = k.bind(self.pdfs, self.periodicity, flags, bh.ubb_velocities, self.kernel_params)
+            self._bound_sweep = k.bind(self.pdfs, self.periodicity, flags, bh.ubb_velocities, self.kernel_params,
+                                       fixed_density=bh.fixed_density)
             self._bound_key = (id(bh._dev), bh._dev is None, tuple(sorted(self.kernel_params.items())),
                                torch.cuda.current_stream().cuda_stream)
         closure = self._kernels[0].update_rule.collision_rule.closure

@@ -623,8 +623,12 @@ void om_periodic_sync(const om_method* m, const om_grid* gr, int pattern, int pr
  * 0 fluid, 1 NoSlip, 2 UBB (velocity ubb_u).  f_out / f_in proxies follow
  * advanced_streaming/indexing.py:12-183; NoSlip boundaryconditions.py:128-139,
  * UBB boundaryconditions.py:794-841. */
+/* Flags: 1 NoSlip, 2 UBB (velocity ubb_u), 6 FixedDensity (density fd_rho).
+ * FixedDensity (boundaryconditions.py:1044-1099): f_in(inv q) = 2 feq_even_q(rho_w, u) - f_out(q),
+ * feq_even the part of the method's equilibrium that is even in u (the mean of directions q and
+ * inv q), u from the fluid cell's outgoing populations with the density replaced by rho_w. */
 void om_boundaries(const om_method* m, const om_grid* gr, int pattern, int prev_parity,
-                   const uint8_t* flags, const double ubb_u[3], double* f) {
+                   const uint8_t* flags, const double ubb_u[3], double fd_rho, double* f) {
     int ooff[QMAX][3], oslot[QMAX], ioff[QMAX][3], islot[QMAX], i;
     int next_parity = 1 - prev_parity;
     for (i = 0; i < m->Q; ++i) {
@@ -651,6 +655,15 @@ void om_boundaries(const om_method* m, const om_grid* gr, int pattern, int prev_
                     rho = m->zero_centered ? 1.0 + s : s;
                 }
                 val = fout - 6.0 * m->w[q] * cu * rho;
+            } else if (fl == 6) {
+                double j[3] = {0.0, 0.0, 0.0}, u[3], feq[QMAX]; int k, d;
+                for (k = 0; k < m->Q; ++k) {
+                    const double fk = f[gidx(gr, x + ooff[k][0], y + ooff[k][1], z + ooff[k][2]) + oslot[k] * gr->s[3]];
+                    for (d = 0; d < 3; ++d) j[d] += m->c[k][d] * fk;
+                }
+                for (d = 0; d < 3; ++d) u[d] = m->compressible ? j[d] / fd_rho : j[d];
+                om_equilibrium(m, fd_rho, u, feq);
+                val = feq[q] + feq[iq] - fout;
             }
             f[gidx(gr, x + ioff[iq][0], y + ioff[iq][1], z + ioff[iq][2]) + islot[iq] * gr->s[3]] = val;
         }
@@ -699,13 +712,14 @@ void om_get_macroscopic(const om_method* m, const om_grid* gr, int pattern, int 
  * and is updated.  For two-field patterns a and b are swapped by pointer; returns 1 if the
  * result ends up in b. */
 int om_run(const om_method* m, const om_grid* gr, int pattern, int* parity, int steps,
-           const int periodic[3], const uint8_t* flags, const double ubb_u[3], double* a, double* b) {
+           const int periodic[3], const uint8_t* flags, const double ubb_u[3], double fd_rho, double* a,
+           double* b) {
     int t, inplace = (pattern == P_AA || pattern == P_ESOTWIST || pattern == P_ESOPULL || pattern == P_ESOPUSH),
         swapped = 0;
     double *src = a, *dst = b;
     for (t = 0; t < steps; ++t) {
         om_periodic_sync(m, gr, pattern, *parity, periodic, src);
-        if (flags) om_boundaries(m, gr, pattern, *parity, flags, ubb_u, src);
+        if (flags) om_boundaries(m, gr, pattern, *parity, flags, ubb_u, fd_rho, src);
         *parity = inplace ? 1 - *parity : *parity;
         om_sweep(m, gr, pattern, *parity, src, inplace ? src : dst, flags, 0);
         if (!inplace) { double* tmp = src; src = dst; dst = tmp; swapped ^= 1; }

@@ -218,8 +218,9 @@ class Oracle:
         return rho, u
 
     def run(self, f, steps, pattern="pull", parity=0, periodic=(True, True, True), flags=None,
-            ubb_velocity=(0.0, 0.0, 0.0), tmp=None):
-        """Runs `steps` time steps.  Returns (field holding the result, new parity)."""
+            ubb_velocity=(0.0, 0.0, 0.0), tmp=None, fixed_density=1.0):
+        """Runs `steps` time steps.  Returns (field holding the result, new parity).  Flags: 1 NoSlip,
+        2 UBB (ubb_velocity), 6 FixedDensity (fixed_density)."""
         g = self._grid(f)
         per = (ctypes.c_int * 3)(*[int(p) for p in periodic])
         par = ctypes.c_int(parity)
@@ -234,11 +235,12 @@ class Oracle:
                 tmp[...] = f
             sw = lib().om_run(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], ctypes.byref(par),
                               steps, per, fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None
-                              else None, self._ptr(ub), self._ptr(f), self._ptr(tmp))
+                              else None, self._ptr(ub), ctypes.c_double(fixed_density), self._ptr(f),
+                              self._ptr(tmp))
             return (tmp if sw else f), par.value
         lib().om_run(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], ctypes.byref(par), steps, per,
                      fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None else None,
-                     self._ptr(ub), self._ptr(f), self._ptr(f))
+                     self._ptr(ub), ctypes.c_double(fixed_density), self._ptr(f), self._ptr(f))
         return f, par.value
 
     def periodic_sync(self, f, pattern="pull", prev_parity=0, periodic=(True, True, True)):
