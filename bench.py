@@ -32,6 +32,7 @@ OMEGA = 1.95
 FORCE = 1e-7
 E2E_SWEEPS = 100          # sweeps per end-to-end call (one LatticeBoltzmannStep.run() in lbmpy terms)
 FALLBACK_HBM_GBS = 6650.0
+METRIC = "D3Q19/D3Q27 GLUPS and % of HBM roofline; FP16-store vs FP32 at equal L2 error"
 
 # DRAM bytes (read + write) per sweep launch from one ncu capture of the same workload, averaged
 # over the launches captured; summaries with their commands are under profiles/.
@@ -240,11 +241,11 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     cells = n[0] * n[1] * n[2]
     value = cells * args.steps / dt / 1e9
-    line = {"impl": "reference", "metric": "D3Q27 cumulant channel GLUPS", "value": value, "unit": "GLUPS",
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GLUPS",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "d3q27-cumulant-aa-channel-256x128x128 (sample: 256x128x8 slab per step)",
+            "config": {"workload": "d3q27-cumulant-aa-channel-256x128x128", "sample": "256x128x8 slab per step",
                        "omega": OMEGA, "force": FORCE, "pattern": "aa", "galilean_correction": True},
             "cpu_baseline": {"value": value, "unit": "GLUPS", "cores": os.cpu_count(), "kind": "port",
                              "sample": "one sweep of a 256x128x8 slab of the channel per step (CPU oracle, "
@@ -392,7 +393,7 @@ def main():
                                        secondary["d3q19-trt-pull-float32-512"]["GLUPS"])
 
     if rank == 0:
-        line = {"metric": "D3Q19/D3Q27 GLUPS and % of HBM roofline; FP16-store vs FP32 at equal L2 error",
+        line = {"metric": METRIC,
                 "value": glups, "unit": "GLUPS", "n_gpus": world,
                 "steps": args.steps, "warmup": warm + (warm % 2), "ms_per_step": ms_per_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
