@@ -158,3 +158,15 @@ def test_plan_create_without_a_device_reports_an_error():
     k = L.create_lb_function(lbm_config=L.LBMConfig(stencil=L.Stencil.D3Q19, relaxation_rate=1.0))
     with pytest.raises(N.LbmError):
         N.Plan(build_desc(k.update_rule, (8, 8, 8), (1, 1, 1), {}))
+
+
+def test_status_and_variant_queries_check_their_arguments():
+    """lbm_plan_status / lbm_sweep_variant refuse NULL plans and outputs before any CUDA call."""
+    v = ctypes.c_uint32(7)
+    assert N.lib().lbm_plan_status(None, ctypes.byref(v), 1) == N.LBM_E_INVALID
+    assert v.value == 7
+    out = ctypes.c_int(-1)
+    strides = N.i64_array((1, 10, 100, 1000))
+    assert N.lib().lbm_sweep_variant(None, None, None, strides, 0, None, ctypes.byref(out)) == N.LBM_E_INVALID
+    assert N.lib().lbm_sweep_variant(None, None, None, strides, 0, None, None) == N.LBM_E_INVALID
+    assert "NULL" in N.last_error()
