@@ -191,31 +191,59 @@ def make_channel(device, shape=SHAPE, seed=0):
     return step
 
 
-def cpu_baseline_sample(seconds_budget=15.0):
-    """The oracle (C, OpenMP, FP64) on a bounded sample of the same channel: a 256 x 128 x 8
-    slab of the channel (periodic x, walls in y, z), timed on all host threads."""
+def _cpu_channel(dtype=np.float32):
+    """The headline channel on the closed-form CPU kernel (oracle/lbm_cpu.c, lbmpy's generated-kernel
+    style: fzyx, one cell per inner iteration vectorised over x, OpenMP over rows), same shape,
+    method, storage type and initial state as the GPU run."""
+    from oracle import cpu as C
     from oracle import oracle as O
-    n = (256, 128, 8)
-    o = O.make("D3Q27", "cumulant", relaxation_rate=OMEGA, compressible=True, galilean_correction=True,
-               force=(FORCE, 0, 0))
-    f = o.new_field(n)
+    orc = O.make("D3Q27", "cumulant", relaxation_rate=OMEGA, compressible=True, galilean_correction=True,
+                 force=(FORCE, 0, 0))
+    fc = C.FastCPU("cumulant", orc, dtype=dtype)
+    n = SHAPE
+    f = orc.new_field(n)
     rng = np.random.default_rng(0)
-    o.set_equilibrium(f, np.ones(n), rng.uniform(-1e-4, 1e-4, n + (3,)), "aa", 1)
+    orc.set_equilibrium(f, np.ones(n), rng.uniform(-1e-4, 1e-4, n + (3,)), "aa", 0)
+    g = fc.new_field(n)
+    g[...] = f
+    del f
     flags = np.zeros((n[0] + 2, n[1] + 2, n[2] + 2), np.uint8)
     flags[:, 0, :] = flags[:, -1, :] = flags[:, :, 0] = flags[:, :, -1] = 1
-    par = 1
-    f, par = o.run(f, 1, "aa", par, periodic=(1, 0, 0), flags=flags)
+    return fc, g, flags
+
+
+def _cpu_info():
+    model = None
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return threads, model
+
+
+def cpu_baseline_sample(seconds_budget=15.0):
+    """The full 256 x 128 x 128 channel (D3Q27 cumulant AA, FP32) on the closed-form CPU kernel,
+    OpenMP on every host thread: sweeps timed until about a third of the budget has passed."""
+    fc, g, flags = _cpu_channel()
+    par = fc.run(g, 2, 1, periodic=(1, 0, 0), flags=flags)[1]      # warm-up
     steps, t0 = 0, time.perf_counter()
     while True:
-        f, par = o.run(f, 2, "aa", par, periodic=(1, 0, 0), flags=flags)
+        par = fc.run(g, 2, par, periodic=(1, 0, 0), flags=flags)[1]
         steps += 2
-        if time.perf_counter() - t0 > seconds_budget / 3 or steps >= 40:
+        if time.perf_counter() - t0 > seconds_budget / 3 or steps >= 200:
             break
     dt = time.perf_counter() - t0
-    cells = n[0] * n[1] * n[2]
-    return {"value": cells * steps / dt / 1e9, "unit": "GLUPS", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{steps} sweeps of a 256x128x8 slab of the channel (D3Q27 cumulant AA, FP64 oracle, "
-                      f"OpenMP)"}
+    cells = SHAPE[0] * SHAPE[1] * SHAPE[2]
+    threads, model = _cpu_info()
+    return {"value": cells * steps / dt / 1e9, "unit": "GLUPS", "cores": threads, "kind": "port",
+            "cpu_model": model,
+            "sample": f"{steps} sweeps of the full 256x128x128 channel (D3Q27 cumulant AA, FP32, closed-form "
+                      f"OpenMP kernel vectorised over x, oracle/lbm_cpu.c)"}
 
 
 def run_reference(args):
@@ -224,32 +252,29 @@ def run_reference(args):
         return
     from oracle import oracle as O
     O.build()
-    n = (256, 128, 8)   # one bounded sample of the channel per step
-    o = O.make("D3Q27", "cumulant", relaxation_rate=OMEGA, compressible=True, galilean_correction=True,
-               force=(FORCE, 0, 0))
-    f = o.new_field(n)
-    rng = np.random.default_rng(0)
-    o.set_equilibrium(f, np.ones(n), rng.uniform(-1e-4, 1e-4, n + (3,)), "aa", 1)
-    flags = np.zeros((n[0] + 2, n[1] + 2, n[2] + 2), np.uint8)
-    flags[:, 0, :] = flags[:, -1, :] = flags[:, :, 0] = flags[:, :, -1] = 1
+    fc, g, flags = _cpu_channel()
     par = 1
     for _ in range(args.warmup):
-        f, par = o.run(f, 1, "aa", par, periodic=(1, 0, 0), flags=flags)
+        par = fc.run(g, 1, par, periodic=(1, 0, 0), flags=flags)[1]
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        f, par = o.run(f, 1, "aa", par, periodic=(1, 0, 0), flags=flags)
+        par = fc.run(g, 1, par, periodic=(1, 0, 0), flags=flags)[1]
     dt = time.perf_counter() - t0
-    cells = n[0] * n[1] * n[2]
+    cells = SHAPE[0] * SHAPE[1] * SHAPE[2]
     value = cells * args.steps / dt / 1e9
+    threads, model = _cpu_info()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GLUPS",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "d3q27-cumulant-aa-channel-256x128x128", "sample": "256x128x8 slab per step",
-                       "omega": OMEGA, "force": FORCE, "pattern": "aa", "galilean_correction": True},
-            "cpu_baseline": {"value": value, "unit": "GLUPS", "cores": os.cpu_count(), "kind": "port",
-                             "sample": "one sweep of a 256x128x8 slab of the channel per step (CPU oracle, "
-                                       "FP64, OpenMP on all host threads)"},
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "d3q27-cumulant-aa-channel-256x128x128", "shape": list(SHAPE),
+                       "omega": OMEGA, "force": FORCE, "pattern": "aa", "galilean_correction": True,
+                       "storage": "float32 zero-centred"},
+            "cpu_baseline": {"value": value, "unit": "GLUPS", "cores": threads, "kind": "port",
+                             "cpu_model": model,
+                             "sample": "one sweep of the full 256x128x128 channel per step (closed-form "
+                                       "OpenMP kernel in lbmpy's generated-kernel style, FP32, all host "
+                                       "threads; lbmpy itself cannot be imported here)"},
             "e2e": {"value": value, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -263,6 +288,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=5000,
+                    help="sweeps of the FP16/BF16/FP32-vs-FP64 accuracy run in `secondary` (0: skip)")
     ap.add_argument("--workload", default="d3q27-cumulant-aa-channel-256x128x128", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     if args.impl == "reference":
@@ -288,7 +315,7 @@ def main():
     headline = args.workload == "d3q27-cumulant-aa-channel-256x128x128"
     batched = args.workload.startswith("batched")
     warm = max(args.warmup, 3)
-    for _ in range(warm + (warm % 2)):
+    for _ in range(warm):
         step.time_step()
     if batched:
         step.run_sweeps(args.steps)          # captures the graph of K launches that is timed below
@@ -391,11 +418,22 @@ def main():
             torch.cuda.empty_cache()
         secondary["fp16_over_fp32"] = (secondary["d3q19-trt-pull-float16-512"]["GLUPS"] /
                                        secondary["d3q19-trt-pull-float32-512"]["GLUPS"])
+        if args.accuracy_steps > 0:
+            # the same box from the same seeded state, stored in each type and in FP64 for the
+            # reference: relative L2 velocity error after accuracy_steps sweeps (config c3: 5000)
+            from lbmpy_b200.precision import precision_study
+            acc = precision_study(512, args.accuracy_steps, args.accuracy_steps,
+                                  storages=("float32", "float16", "bfloat16"), device=device, log=lambda *_: None)
+            for st in ("float32", "float16", "bfloat16"):
+                secondary[f"d3q19-trt-pull-{st}-512"]["l2_vs_fp64"] = acc[st]["final_l2_velocity_error"]
+                secondary[f"d3q19-trt-pull-{st}-512"]["max_ke_rel_error"] = acc[st]["max_ke_rel_error"]
+            secondary["accuracy_steps"] = args.accuracy_steps
+            torch.cuda.empty_cache()
 
     if rank == 0:
         line = {"metric": METRIC,
                 "value": glups, "unit": "GLUPS", "n_gpus": world,
-                "steps": args.steps, "warmup": warm + (warm % 2), "ms_per_step": ms_per_step,
+                "steps": args.steps, "warmup": warm, "ms_per_step": ms_per_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": {8: "f64", 4: "f32", 2: "f32 (16-bit storage)"}[itemsize], "data": "synthetic",
                 "config": {"workload": args.workload, "cells": cells, "populations": q_pop,

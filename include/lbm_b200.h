@@ -148,8 +148,9 @@ int lbm_reduce_conserved(const LbmPlan* plan, const void* pdfs, const int64_t st
  * 2048 x 5 doubles (80 KiB per GPU, resident until exit), calling no cudaMalloc / cudaFree.
  * No counterpart in the reference.  Fails with LBM_E_INVALID if the launch would need more than
  * 2048 partial sums (more than 512 SMs).  Calls that overlap on the GPU share the array and race.
- * The first call on a device resolves the array's address; make it before any stream capture.
- * Waits for its result. */
+ * The first call on a device resolves the array's address and, with lazy module loading, may
+ * load the library's module there (reserving the 80 KiB array and the code): make it at start-up.
+ * Waits for its result, so it cannot be captured into a CUDA graph. */
 int lbm_reduce_conserved_noalloc(const LbmPlanDesc* desc, const void* pdfs, const int64_t strides[4],
                                  const uint8_t* flags, int prev_parity, double out[5], void* stream);
 

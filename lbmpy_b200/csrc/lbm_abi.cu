@@ -835,6 +835,7 @@ int lbm_reduce_conserved(const LbmPlan* p, const void* pdfs, const int64_t strid
     a.g.flags = flags;
     const int pat = pattern_kind(p, prev_parity ? 1 : 0);
     ReduceLauncher L = p->q == 19 ? reduce_launcher_q<19>(p->store, pat) : reduce_launcher_q<27>(p->store, pat);
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no reduction kernel for this storage type / pattern");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e = L(a, p->red_blocks, p->partial, s);
     if (e != cudaSuccess) return cuda_fail(e, "reduction launch");
@@ -1139,8 +1140,11 @@ int lbm_batch_destroy(LbmBatch* b) {
 // array exists once per GPU that loads the library, for the life of the process.  Every call
 // overwrites the partials it reads, so no state carries over between calls, but calls that
 // overlap on the GPU (different streams, or concurrent host threads) share the array and race.
-// The first call on a device resolves the array's device address (cudaGetSymbolAddress); make
-// that first call before any stream capture on that device.
+// The first call on a device resolves the array's device address (cudaGetSymbolAddress); with
+// lazy module loading that first call may also load the library's module on the device, which
+// reserves the array itself and the code.  Make that first call at start-up, before the caller's
+// memory budget is fixed.  The call waits for its result (cudaStreamSynchronize), so it cannot
+// be recorded into a CUDA graph.
 static constexpr int LBM_NOALLOC_MAX_BLOCKS = 2048;
 static __device__ __align__(256) double g_noalloc_scratch[LBM_NOALLOC_MAX_BLOCKS * 5 + 5];
 
@@ -1174,7 +1178,7 @@ extern "C" int lbm_reduce_conserved_noalloc(const LbmPlanDesc* desc, const void*
     cudaError_t e = cudaGetDevice(&p.device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     p.q = desc->stencil;
-    p.mk = desc->method == LBM_METHOD_MRT ? MK_MRT : (desc->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
+    p.mk = method_kind(desc);
     p.store = desc->store_dtype;
     fill_physics(&p, desc);
     MacroArgs a;

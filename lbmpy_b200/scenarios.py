@@ -12,7 +12,7 @@ def create_fully_periodic_flow(initial_velocity, periodicity_in_kernel=False, lb
     """Periodic box initialised in equilibrium with `initial_velocity` ([x, y, z, 3]); scenarios.py:37-69.
     Periodicity is an index wrap in the sweep whether or not `periodicity_in_kernel` is set."""
     if parallel:
-        raise NotImplementedError("use lbmpy_b200.decomposition for multi-GPU domains")
+        raise NotImplementedError("use lbmpy_b200.distributed (DistributedLatticeBoltzmannStep) for multi-GPU domains")
     initial_velocity = np.asarray(initial_velocity)
     domain_size = initial_velocity.shape[:-1]
     step = LatticeBoltzmannStep(domain_size=domain_size, periodicity=True, lbm_kernel=lbm_kernel,
@@ -45,7 +45,7 @@ def create_channel(domain_size=None, force=None, pressure_difference=None, u_max
         raise NotImplementedError("pressure- and velocity-driven channels need FixedDensity / inflow profiles, "
                                   "which are not built")
     if parallel:
-        raise NotImplementedError("use lbmpy_b200.decomposition for multi-GPU domains")
+        raise NotImplementedError("use lbmpy_b200.distributed (DistributedLatticeBoltzmannStep) for multi-GPU domains")
     wall_boundary = wall_boundary or NoSlip()
     kwargs["force"] = (force, 0, 0)
     step = LatticeBoltzmannStep(domain_size=domain_size, periodicity=(True, False, False),

@@ -55,6 +55,8 @@ typedef struct {
     double sgs_c;
     double shear_rate;
     float mlp[MLP_NPARAM];    /* sgs == 2: W1[10][32] b1[32] W2[32][32] b2[32] W3[32] b3 scale */
+    int discrete_eq;          /* moment based: 1 = discrete Maxwellian (maxwellian_equilibrium.py:64-104,
+                                 equilibrium/discrete_hydro_maxwellian.py:9-96), 0 = continuous */
 } om_method;
 
 typedef struct {
@@ -164,6 +166,19 @@ static double maxwell_raw(const int e[3], const double u[3], int order, double c
 /* Equilibrium value of polynomial moment k in the method's storage convention. */
 static double eq_moment(const om_method* m, int k, double rho, double drho, const double u[3]) {
     double pu = 0.0, p0 = 0.0, zero[3] = {0, 0, 0}, base; int t;
+    if (m->discrete_eq && m->kind == 0) {
+        /* moment k of the discrete populations w_i rho (1 + c.u/cs2 + (c.u)^2/(2 cs4) - u.u/(2 cs2))
+         * (compressible) or w_i rho + w_i (...) (incompressible), minus w_i in delta form */
+        double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2], r = 0.0; int i;
+        for (i = 0; i < m->Q; ++i) {
+            double cu = m->c[i][0] * u[0] + m->c[i][1] * u[1] + m->c[i][2] * u[2];
+            double poly = 3.0 * cu + 4.5 * cu * cu - 1.5 * uu, fe;
+            fe = m->compressible ? m->w[i] * rho * (1.0 + poly) : m->w[i] * (rho + poly);
+            if (m->delta_eq) fe -= m->w[i];
+            r += m->M[k][i] * fe;
+        }
+        return r;
+    }
     for (t = 0; t < m->nterms[k]; ++t) {
         pu += m->tcoef[k][t] * maxwell_raw(m->texp[k][t], u, m->eq_order, 1.0 / 3.0);
         p0 += m->tcoef[k][t] * maxwell_raw(m->texp[k][t], zero, m->eq_order, 1.0 / 3.0);

@@ -47,6 +47,7 @@ class OmMethod(ctypes.Structure):
         ("sgs_c", ctypes.c_double),
         ("shear_rate", ctypes.c_double),
         ("mlp", ctypes.c_float * MLP_NPARAM),
+        ("discrete_eq", ctypes.c_int),
     ]
 
 
@@ -143,6 +144,7 @@ class Oracle:
             w = np.asarray(method.mlp, dtype=np.float32).reshape(-1)
             assert w.size == MLP_NPARAM, f"closure parameters: {w.size} != {MLP_NPARAM}"
             ctypes.memmove(ctypes.addressof(m.mlp), w.ctypes.data, w.nbytes)
+        m.discrete_eq = int(not method.continuous_equilibrium)
         self._m = m
         self.M = np.array([[float(v) for v in r] for r in M])
         self.Minv = np.array([[float(v) for v in r] for r in Minv])

@@ -335,6 +335,7 @@ class OracleMethod:
     sgs_constant: float = 0.12
     shear_rate: float = 0.0
     mlp: object = None            # learned-closure parameters (float32 array) when sgs == SGS_MLP
+    continuous_equilibrium: bool = True   # SRT/TRT/MRT: False = discrete Maxwellian
 
     @property
     def Q(self):
@@ -348,7 +349,8 @@ class OracleMethod:
 def resolve(stencil: str, method: str, relaxation_rate=None, relaxation_rates=None,
             compressible=False, zero_centered=True, delta_equilibrium=None,
             equilibrium_order=2, force=(0.0, 0.0, 0.0), force_model=None,
-            galilean_correction=False, smagorinsky=None, mlp=None) -> OracleMethod:
+            galilean_correction=False, smagorinsky=None, mlp=None,
+            continuous_equilibrium=True) -> OracleMethod:
     """Follows ``LBMConfig.__post_init__`` (creationfunctions.py:347-484) and
     ``create_lb_method`` (creationfunctions.py:773-868) for SRT/TRT/MRT/CUMULANT."""
     method = method.lower()
@@ -414,4 +416,5 @@ def resolve(stencil: str, method: str, relaxation_rate=None, relaxation_rates=No
                         zero_centered=bool(zero_centered), delta_equilibrium=bool(delta_equilibrium),
                         equilibrium_order=equilibrium_order, force_model=fm, force=force,
                         galilean_correction=bool(galilean_correction), sgs=sgs, sgs_constant=c_sgs,
-                        shear_rate=float(shear), mlp=mlp)
+                        shear_rate=float(shear), mlp=mlp,
+                        continuous_equilibrium=bool(continuous_equilibrium) or kind != KIND_MOMENT)

@@ -28,4 +28,6 @@ def main(reference_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_orderings.py <path to the lbmpy checkout>")
+    main(sys.argv[1])

@@ -1,0 +1,42 @@
+"""The CUDA sweep reproduces lbmpy's own stored states directly (no oracle in between).
+
+lbmpy's regression files hold the D3Q19 lid-driven cavity (16 x 17 x 18, lid 0.005 on N, NoSlip
+W/E/S/T/B) after 100 steps of TRT with rates (1.8, 1.3), the discrete Maxwellian equilibrium and
+the Luo force (1e-4, -2e-5, 1.24e-5), started from rest.  tests/test_golden_states.py identifies
+those parameters on the CPU oracle; here the same run goes through the lbmpy-compatible API and
+the C ABI.  The compressible file stores absolute PDFs: the sweep stores f - w, so w is added
+back before the comparison.
+"""
+import numpy as np
+import pytest
+
+import lbmpy_b200 as L
+from lbmpy_b200.boundaries import NoSlip, UBB, slice_from_direction
+from tests.test_golden_states import TRT_FORCE, TRT_RATES, _sample
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-13), ("float32", 2e-6)])
+@pytest.mark.parametrize("compressible", [True, False])
+def test_d3q19_trt_lid_driven_cavity_matches_lbmpy(cuda, compressible, dtype, tol):
+    """Pull streaming, as lbmpy ran it: the stored field is the post-collision state of every
+    cell, which the in-place patterns keep in other slots."""
+    name = f"LidDrivenCavity_TRT_luo_{'compressible' if compressible else 'incompressible'}"
+    shape, idx, ref = _sample(name)
+    n = shape[:3]
+    step = L.LatticeBoltzmannStep(domain_size=n, periodicity=False, stencil=L.Stencil.D3Q19,
+                                  method=L.Method.TRT, relaxation_rates=TRT_RATES, compressible=compressible,
+                                  continuous_equilibrium=False, force=TRT_FORCE, force_model="luo",
+                                  config=L.CreateKernelConfig(data_type=dtype))
+    step.boundary_handling.set_boundary(UBB((0.005, 0.0, 0.0)), slice_from_direction("N", 3))
+    for d in ("W", "E", "S", "T", "B"):
+        step.boundary_handling.set_boundary(NoSlip(), slice_from_direction(d, 3))
+    step.set_pdf_fields_from_macroscopic_values()
+    step.run(100)
+    got = step.pdfs[1:-1, 1:-1, 1:-1].detach().double().cpu().numpy()
+    if compressible:
+        got = got + np.asarray(step.method.weights, np.float64)
+    got = np.ascontiguousarray(got).reshape(-1)[idx]
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() < tol * scale

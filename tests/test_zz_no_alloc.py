@@ -63,11 +63,14 @@ def test_noalloc_reduction_matches_allocating_entry_point(cuda, setup):
     got2, ref2 = _reduce_both(step)
     np.testing.assert_allclose(got2, ref2, rtol=1e-12, atol=1e-15)
     assert not np.allclose(got1[1:], got2[1:], rtol=0, atol=0) or setup.startswith("d3q19")
-    # with every kernel of this configuration loaded, a further call leaves free device memory as is
+    # with every kernel of this configuration loaded, a further call reserves nothing through torch's
+    # allocator, and free device memory moves by no more than other users of a shared GPU could
+    reserved_before = torch.cuda.memory_reserved()
     free_before = torch.cuda.mem_get_info()[0]
     got3, ref3 = _reduce_both(step)
     torch.cuda.synchronize()
-    assert torch.cuda.mem_get_info()[0] == free_before
+    assert torch.cuda.memory_reserved() == reserved_before
+    assert abs(torch.cuda.mem_get_info()[0] - free_before) <= 4 << 20
     np.testing.assert_array_equal(got3, got2)
 
 
