@@ -16,8 +16,8 @@
  * must be 1 and sy, sz, sq are passed in `strides` = {1, sy, sz, sq}.
  *
  * Flag field (optional): uint8 over the ghost-inclusive domain, x fastest, contiguous:
- * index x + (nx+2)*(y + (ny+2)*z).  Low 3 bits: 0 fluid, 1 NoSlip, 2..5 UBB number 0..3,
- * 6 FixedDensity (density `fixed_density` of the plan);
+ * index x + (nx+2)*(y + (ny+2)*z).  Low 4 bits: 0 fluid, 1 NoSlip, 2..5 UBB number 0..3,
+ * 6 / 7 FixedDensity (density `fixed_density` / `fixed_density1` of the plan);
  * bit 7 marks fluid cells with a boundary neighbour (lbm_flags_finalize sets it).
  */
 #ifndef LBM_B200_H
@@ -72,6 +72,14 @@ typedef struct LbmPlanDesc {
     int32_t periodic[3];
     double fixed_density;       /* wall density of FixedDensity cells (flag type 6); 0: none
                                    (boundaries/boundaryconditions.py:1044-1099) */
+    double fixed_density1;      /* wall density of FixedDensity cells of flag type 7 (a second outlet
+                                   or inlet density, create_channel(pressure_difference=...),
+                                   scenarios.py:137-142); 0: none */
+    double ubb_density[4];      /* prescribed wall density of UBB number u for compressible methods;
+                                   0: the fluid cell's density (UBB(density=...),
+                                   boundaries/boundaryconditions.py:824-830) */
+    uint32_t ubb_adapt_mask;    /* bit u: UBB number u shifts its wall velocity by -F/(2 rho_ref)
+                                   (UBB(adapt_velocity_to_force=True), :790-794) */
 } LbmPlanDesc;
 
 typedef struct LbmPlan LbmPlan;
@@ -153,6 +161,16 @@ int lbm_reduce_conserved(const LbmPlan* plan, const void* pdfs, const int64_t st
  * Waits for its result, so it cannot be captured into a CUDA graph. */
 int lbm_reduce_conserved_noalloc(const LbmPlanDesc* desc, const void* pdfs, const int64_t strides[4],
                                  const uint8_t* flags, int prev_parity, double out[5], void* stream);
+
+/* Per-link wall velocities of UBB numbers in `link_mask` (bit u: UBB number u), for velocity
+ * profiles that vary from link to link: lbmpy's UBB(velocity=callback) fills one velocity per
+ * boundary link through its index array (boundaries/boundaryconditions.py:747-799,
+ * geometry.py:36-86).  cell_block: int32 per interior cell, x fastest, the block of the cell's links
+ * or -1; link_velocity: double [n_blocks][Q][3], entry [b][q] the velocity of the link from the
+ * cell in direction q (towards the wall).  Device memory owned by the caller, kept by the plan
+ * (pass link_mask 0 to detach).  The other UBB numbers keep their constant velocities. */
+int lbm_plan_set_ubb_links(LbmPlan* plan, const int32_t* cell_block, const double* link_velocity,
+                           int64_t n_blocks, uint32_t link_mask);
 
 /* Sets bit 7 on every fluid cell of `flags` (device, layout above) that has a boundary
  * neighbour along the plan's stencil, honouring periodicity.  Replaces the link-list setup of

@@ -32,6 +32,9 @@ struct LbmPlan {
     uint32_t* rowmask;     // row summary of the flag field last finalized with this plan
     mutable const uint8_t* rowmask_flags;  // that flag field (sweeps given it use the summary)
     void* ubb_rho;         // compressible + moving UBB walls: density gathered before the sweep
+    const int* ubb_block;  // per-link UBB velocities (lbm_plan_set_ubb_links), caller-owned
+    const double* ubb_link_vel;
+    uint32_t ubb_link_mask;
     Physics phys;
     double* partial;       // reduction scratch: RED_BLOCKS * 5 doubles
     double* red_out;       // 5 doubles on the device
@@ -392,17 +395,24 @@ UbbLauncher ubb_launcher_q(int store, int pat) {
     return nullptr;
 }
 
-// The compressible UBB of a moving wall needs the cell's previous-step density.
-bool needs_ubb_density(const LbmPlanDesc* d) {
+// The compressible UBB of a moving wall needs the cell's previous-step density (unless the wall
+// density is prescribed): a non-zero constant velocity, per-link velocities, or a wall velocity
+// shifted by the force.
+bool needs_ubb_density(const LbmPlanDesc* d, uint32_t link_mask) {
     if (!d->compressible) return false;
-    for (int u = 0; u < 4; ++u)
+    const bool force = d->force[0] != 0.0 || d->force[1] != 0.0 || d->force[2] != 0.0;
+    for (int u = 0; u < 4; ++u) {
+        if (d->ubb_density[u] > 0.0) continue;
+        if ((link_mask >> u) & 1u) return true;
+        if (force && ((d->ubb_adapt_mask >> u) & 1u)) return true;
         for (int k = 0; k < 3; ++k)
             if (d->ubb_velocity[u][k] != 0.0) return true;
+    }
     return false;
 }
 
 int ensure_ubb_buffer(LbmPlan* p) {
-    if (!needs_ubb_density(&p->desc) || p->ubb_rho != nullptr) return LBM_OK;
+    if (!needs_ubb_density(&p->desc, p->ubb_link_mask) || p->ubb_rho != nullptr) return LBM_OK;
     const size_t n = size_t(p->desc.dims[0]) * p->desc.dims[1] * p->desc.dims[2];
     cudaError_t e = cudaMalloc(&p->ubb_rho, n * (p->store == ST_F64 ? 8 : 4));
     if (e != cudaSuccess) {
@@ -468,6 +478,10 @@ int fill_physics(LbmPlan* p, const LbmPlanDesc* d) {
         for (int k = 0; k < 3; ++k) ph.ubb[u][k] = d->ubb_velocity[u][k];
     if (d->method == LBM_METHOD_SRT) ph.rates[1] = ph.rates[0];
     ph.fixed_density = d->fixed_density;
+    ph.fixed_density1 = d->fixed_density1;
+    for (int u = 0; u < MAX_UBB; ++u) ph.ubb_density[u] = d->ubb_density[u];
+    ph.ubb_adapt_mask = d->ubb_adapt_mask & 0xfu;
+    ph.ubb_link_mask = p->ubb_link_mask;
     return LBM_OK;
 }
 
@@ -517,7 +531,14 @@ int validate_desc(const LbmPlanDesc* d) {
         return fail(LBM_E_UNSUPPORTED, "the learned closure is built for FP32 and FP64 storage");
     if (d->sgs == LBM_SGS_MLP && d->pattern != LBM_PATTERN_PULL && d->pattern != LBM_PATTERN_AA)
         return fail(LBM_E_UNSUPPORTED, "the learned closure is built for the pull and AA patterns");
-    if (!(d->fixed_density >= 0.0)) return fail(LBM_E_INVALID, "fixed_density must be >= 0 (0: no FixedDensity cells)");
+    if (!(d->fixed_density >= 0.0) || !(d->fixed_density1 >= 0.0))
+        return fail(LBM_E_INVALID, "fixed_density must be >= 0 (0: no FixedDensity cells)");
+    if (d->fixed_density1 > 0.0 && d->force_model != LBM_FORCE_NONE)
+        return fail(LBM_E_UNSUPPORTED, "FixedDensity boundaries are built for force-free methods");
+    for (int u = 0; u < 4; ++u)
+        if (!(d->ubb_density[u] >= 0.0))
+            return fail(LBM_E_INVALID, "ubb_density must be >= 0 (0: the density of the fluid cell)");
+    if (d->ubb_adapt_mask & ~0xfu) return fail(LBM_E_INVALID, "ubb_adapt_mask has bits beyond UBB number 3");
     if (d->fixed_density > 0.0 && d->force_model != LBM_FORCE_NONE)
         return fail(LBM_E_UNSUPPORTED, "FixedDensity boundaries are built for force-free methods");
     for (int k = 0; k < 3; ++k)
@@ -576,6 +597,9 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
         if (p->ns < 2) p->ns = 2;
         if (p->ns > STAGED_MAX_NS) p->ns = STAGED_MAX_NS;
     }
+    p->ubb_block = nullptr;
+    p->ubb_link_vel = nullptr;
+    p->ubb_link_mask = 0;
     fill_physics(p, desc);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
@@ -673,8 +697,10 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
     a.pad_ = 0;
     a.ubb_rho = nullptr;
     a.status = p->status;
+    a.ubb_block = p->ubb_block;
+    a.ubb_link_vel = p->ubb_link_vel;
     if (flags != nullptr && flags == p->rowmask_flags) a.g.rowmask = p->rowmask;
-    if (flags != nullptr && p->ubb_rho != nullptr && needs_ubb_density(&p->desc)) {
+    if (flags != nullptr && p->ubb_rho != nullptr && needs_ubb_density(&p->desc, p->ubb_link_mask)) {
         UbbLauncher U = p->q == 19 ? ubb_launcher_q<19>(p->store, pat) : ubb_launcher_q<27>(p->store, pat);
         if (U == nullptr) return fail(LBM_E_UNSUPPORTED, "no wall-density kernel for this storage type / pattern");
         dim3 ug, ub;
@@ -683,7 +709,7 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
         if (e != cudaSuccess) return cuda_fail(e, "wall-density launch");
         a.ubb_rho = p->ubb_rho;
     }
-    if (flags != nullptr && p->desc.fixed_density > 0) {
+    if (flags != nullptr && (p->desc.fixed_density > 0 || p->desc.fixed_density1 > 0)) {
         SweepLauncher F = fixed_density_launcher(p, pat);
         if (F == nullptr) return fail(LBM_E_UNSUPPORTED, "no FixedDensity kernel for this storage type / pattern");
         dim3 fg, fb;
@@ -886,6 +912,24 @@ int lbm_flags_finalize(const LbmPlan* p, uint8_t* flags, void* stream) {
     return LBM_OK;
 }
 
+int lbm_plan_set_ubb_links(LbmPlan* p, const int32_t* cell_block, const double* link_velocity, int64_t n_blocks,
+                           uint32_t link_mask) {
+    if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
+    int rc;
+    if ((rc = check_device(p))) return rc;
+    if (link_mask & ~0xfu) return fail(LBM_E_INVALID, "link_mask has bits beyond UBB number 3");
+    if (link_mask != 0) {
+        if ((rc = check_device_ptr(p, cell_block, "cell_block", false))) return rc;
+        if ((rc = check_device_ptr(p, link_velocity, "link_velocity", false))) return rc;
+        if (n_blocks < 1) return fail(LBM_E_INVALID, "n_blocks must be positive when link_mask is set");
+    }
+    p->ubb_block = link_mask ? reinterpret_cast<const int*>(cell_block) : nullptr;
+    p->ubb_link_vel = link_mask ? link_velocity : nullptr;
+    p->ubb_link_mask = link_mask;
+    p->phys.ubb_link_mask = link_mask;
+    return ensure_ubb_buffer(p);
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------------------
@@ -925,6 +969,9 @@ void domain_plan(const LbmPlanDesc* common, const LbmDomainDesc& d, int device, 
     p.store = common->store_dtype;
     p.partial = nullptr;
     p.red_out = nullptr;
+    p.ubb_block = nullptr;
+    p.ubb_link_vel = nullptr;
+    p.ubb_link_mask = 0;
     fill_physics(&p, &p.desc);
 }
 
@@ -1003,7 +1050,7 @@ int lbm_batch_create(const LbmPlanDesc* common, const LbmDomainDesc* domains, in
             return fail(LBM_E_INVALID, "domain %d: flags_offset must be >= 0 or -1", k);
         }
         if (!cumulant_high_orders_relax_to_equilibrium(&pk.desc)) all_cum1 = false;
-        if (needs_ubb_density(&pk.desc) && d.flags_offset >= 0)
+        if (needs_ubb_density(&pk.desc, 0) && d.flags_offset >= 0)
             return fail(LBM_E_UNSUPPORTED, "domain %d: moving UBB walls of a compressible method are not built "
                         "for batches", k);
         cells += int64_t(d.dims[0]) * d.dims[1] * d.dims[2];

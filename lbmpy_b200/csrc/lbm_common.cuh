@@ -30,15 +30,19 @@ LBM_HD constexpr bool lehmann_even(int x, int y, int z) {
 }
 enum ForceKind : int { FM_NONE = 0, FM_GUO = 1, FM_CENTRAL = 2, FM_SIMPLE = 3, FM_LUO = 4 };
 
-// Cell flags (uint8, ghost-layered domain): low 3 bits = cell type, bit 7 = fluid cell with at
+// Cell flags (uint8, ghost-layered domain): low 4 bits = cell type, bit 7 = fluid cell with at
 // least one boundary neighbour.  Type 0 fluid, 1 NoSlip, 2..5 UBB number (type - 2),
-// 6 FixedDensity.
-constexpr int FLAG_TYPE_MASK = 7;
+// 6 / 7 FixedDensity with the plan's first / second density.
+constexpr int FLAG_TYPE_MASK = 15;
 constexpr int FLAG_NEAR_WALL = 128;
 constexpr int FLAG_NOSLIP = 1;
 constexpr int FLAG_UBB0 = 2;
-constexpr int FLAG_FIXED_DENSITY = 6;
 constexpr int MAX_UBB = 4;
+constexpr int FLAG_FIXED_DENSITY = 6;
+constexpr int FLAG_FIXED_DENSITY1 = 7;
+
+LBM_HD constexpr bool flag_is_ubb(int t) { return t >= FLAG_UBB0 && t < FLAG_UBB0 + MAX_UBB; }
+LBM_HD constexpr bool flag_is_fixed_density(int t) { return t == FLAG_FIXED_DENSITY || t == FLAG_FIXED_DENSITY1; }
 
 template <int Q> struct Lat;
 
@@ -114,7 +118,11 @@ struct Physics {
     uint32_t sgs_mask;     // moments (or TRT parts) whose rate is the shear rate
     int galilean;
     double ubb[MAX_UBB][3];
-    double fixed_density;  // wall density of FixedDensity cells (0: none)
+    double fixed_density;  // wall density of FixedDensity cells of type 6 (0: none)
+    double fixed_density1; // wall density of FixedDensity cells of type 7 (0: none)
+    double ubb_density[MAX_UBB];  // prescribed wall density of UBB number u (0: the fluid cell's density)
+    unsigned ubb_link_mask;       // bit u: UBB number u takes per-link velocities (SweepArgs::ubb_link_vel)
+    unsigned ubb_adapt_mask;      // bit u: the wall velocity is shifted by -F / (2 rho_ref)
 };
 
 struct Grid {
@@ -140,6 +148,11 @@ struct SweepArgs {
     int pad_;
     const void* ubb_rho;   // compressible moving walls: previous-step density of the cells next to them
     unsigned* status;      // device status word of the plan (STATUS_* bits), or nullptr
+    // Per-link UBB velocities: block index of each interior cell (x fastest, -1: none) and, per
+    // block, the velocity of the link in each direction q (pointing from the fluid cell to the
+    // wall, lbmpy's `dir`): ubb_link_vel[(block * Q + q) * 3 + k].
+    const int* ubb_block;
+    const double* ubb_link_vel;
 };
 
 // Whether interior row (y, z) may hold a cell with a non-zero flag.

@@ -105,20 +105,30 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
 #pragma unroll
     for (int i = 1; i < Q; ++i) {
         const int bt = g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK;
-        if (bt == 0 || bt == FLAG_FIXED_DENSITY) continue;   // FixedDensity: written by k_fixed_density
+        if (bt == 0 || flag_is_fixed_density(bt)) continue;   // FixedDensity: written by k_fixed_density
         // f_out(x, inv i): where the previous step wrote direction inv(i) of this cell
         const int j = L::inv(i);
         const int off = nb.off(PA::template woff<Q>(j, 0), PA::template woff<Q>(j, 1), PA::template woff<Q>(j, 2));
         R v = Conv<S, R>::ld(src + eidx(PA::template wslot<Q>(j) * g.sq, cell + off));
-        if (bt >= FLAG_UBB0) {
-            const double* uw = a.p.ubb[bt - FLAG_UBB0];
-            // compressible: the cell's density at the previous step, gathered before the sweep
-            // (k_ubb_density; in-place sweeps overwrite the values it is summed from).  Interior
-            // cell indices fit 32 bits (the host bounds the field below 2^32 elements).
-            const R rho = (a.p.compressible && a.ubb_rho != nullptr)
-                              ? static_cast<const R*>(a.ubb_rho)[x + g.nx * (y + g.ny * z)]
-                              : R(1);
-            const R cu = R(L::cx(i)) * R(uw[0]) + R(L::cy(i)) * R(uw[1]) + R(L::cz(i)) * R(uw[2]);
+        if (flag_is_ubb(bt)) {
+            const int u = bt - FLAG_UBB0;
+            const double* uw = a.p.ubb[u];
+            // Interior cell indices fit 32 bits (the host bounds the field below 2^32 elements).
+            const int icell = x + g.nx * (y + g.ny * z);
+            if ((a.p.ubb_link_mask >> u) & 1u)   // per-link velocity of the link x -> x - c_i (dir inv i)
+                uw = a.ubb_link_vel + (size_t(a.ubb_block[icell]) * Q + size_t(L::inv(i))) * 3;
+            // compressible: the prescribed wall density, else the cell's density at the previous
+            // step, gathered before the sweep (k_ubb_density; in-place sweeps overwrite the
+            // values it is summed from)
+            const R rho = !a.p.compressible ? R(1)
+                          : a.p.ubb_density[u] > 0.0 ? R(a.p.ubb_density[u])
+                          : a.ubb_rho != nullptr ? static_cast<const R*>(a.ubb_rho)[icell] : R(1);
+            R ux = R(uw[0]), uy = R(uw[1]), uz = R(uw[2]);
+            if ((a.p.ubb_adapt_mask >> u) & 1u) {   // the equilibrium velocity of the wall
+                const R h = R(0.5) / rho;
+                ux -= h * R(a.p.force[0]); uy -= h * R(a.p.force[1]); uz -= h * R(a.p.force[2]);
+            }
+            const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
             v += R(6) * R(L::w(i)) * cu * rho;
         }
         f[i] = v;
@@ -215,7 +225,7 @@ __global__ void __launch_bounds__(256) k_ubb_density(const SweepArgs a, R* rho_o
     bool moving = false;
 #pragma unroll
     for (int i = 1; i < Q; ++i)
-        if ((g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK) >= FLAG_UBB0) moving = true;
+        if (flag_is_ubb(g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK)) moving = true;
     if (!moving) return;
     NbrOffsets nb;
     nb.init(g, x, y, z);
@@ -351,11 +361,13 @@ __global__ void __launch_bounds__(256) k_fixed_density(const SweepArgs a) {
         gf.sz = g.fsz;
         fo.init(gf, x, y, z);
     }
-    bool any = false;
+    unsigned types = 0;   // bit 0: a link to a type-6 cell, bit 1: to a type-7 cell
 #pragma unroll
-    for (int i = 1; i < Q; ++i)
-        if ((g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK) == FLAG_FIXED_DENSITY) any = true;
-    if (!any) return;
+    for (int i = 1; i < Q; ++i) {
+        const int t = g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK;
+        if (flag_is_fixed_density(t)) types |= 1u << (t - FLAG_FIXED_DENSITY);
+    }
+    if (!types) return;
     NbrOffsets nb;
     nb.init(g, x, y, z);
     const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
@@ -370,16 +382,21 @@ __global__ void __launch_bounds__(256) k_fixed_density(const SweepArgs a) {
         jy += R(L::cy(k)) * out[k];
         jz += R(L::cz(k)) * out[k];
     }
-    const R rw = R(a.p.fixed_density);
-    const R s = a.p.compressible ? R(1) / rw : R(1);
-    R feq[Q];
-    equilibrium<Q, R, EQ>(feq, rw, jx * s, jy * s, jz * s, a.p);
+#pragma unroll 1
+    for (int t = 0; t < 2; ++t) {
+        if (!((types >> t) & 1u)) continue;
+        const R rw = R(t == 0 ? a.p.fixed_density : a.p.fixed_density1);
+        const R s = a.p.compressible ? R(1) / rw : R(1);
+        R feq[Q];
+        equilibrium<Q, R, EQ>(feq, rw, jx * s, jy * s, jz * s, a.p);
 #pragma unroll
-    for (int i = 1; i < Q; ++i) {
-        if ((g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK) != FLAG_FIXED_DENSITY) continue;
-        const int q = L::inv(i);
-        const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
-        Conv<S, R>::st(f + eidx(A::template rslot<Q>(i) * g.sq, cell + off), feq[q] + feq[i] - out[q]);
+        for (int i = 1; i < Q; ++i) {
+            if ((g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK) != FLAG_FIXED_DENSITY + t)
+                continue;
+            const int q = L::inv(i);
+            const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
+            Conv<S, R>::st(f + eidx(A::template rslot<Q>(i) * g.sq, cell + off), feq[q] + feq[i] - out[q]);
+        }
     }
 }
 

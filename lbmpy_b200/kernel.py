@@ -58,9 +58,11 @@ def free_parameters(update_rule) -> set:
 
 
 def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None,
-               rates_needed: bool = True, fixed_density=None) -> N.LbmPlanDesc:
+               rates_needed: bool = True, fixed_density=None, ubb_options=None) -> N.LbmPlanDesc:
     """Resolves an update rule plus parameter values into the C plan descriptor.  Plans that only
-    run the getter / setter do not need relaxation rates (rates_needed=False)."""
+    run the getter / setter do not need relaxation rates (rates_needed=False).  ubb_options:
+    {"densities": prescribed wall density per UBB number (0: none), "adapt_mask": bit u set when
+    UBB number u adapts its velocity to the force}."""
     rule = update_rule.collision_rule
     m = rule.method
     d = N.LbmPlanDesc()
@@ -107,7 +109,14 @@ def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None,
         vel = list(vel) + [0.0] * 3
         for k in range(3):
             d.ubb_velocity[u][k] = float(vel[k])
-    d.fixed_density = float(fixed_density) if fixed_density is not None else 0.0
+    if fixed_density is not None:
+        fd = list(fixed_density) if isinstance(fixed_density, (tuple, list)) else [fixed_density]
+        d.fixed_density = float(fd[0] or 0.0)
+        d.fixed_density1 = float(fd[1] or 0.0) if len(fd) > 1 else 0.0
+    if ubb_options:
+        for u, rho in enumerate(list(ubb_options.get("densities", ()))[:4]):
+            d.ubb_density[u] = float(rho or 0.0)
+        d.ubb_adapt_mask = int(ubb_options.get("adapt_mask", 0))
     for k in range(3):
         d.dims[k] = int(dims[k])
         d.periodic[k] = int(bool(periodic[k]))
@@ -168,9 +177,9 @@ class LbKernel:
     def q(self):
         return self.method.stencil.Q
 
-    def plan(self, dims, periodic, params=None, ubb_velocities=None, fixed_density=None) -> N.Plan:
+    def plan(self, dims, periodic, params=None, ubb_velocities=None, fixed_density=None, ubb_options=None) -> N.Plan:
         desc = build_desc(self.update_rule, dims, periodic, params or {}, ubb_velocities,
-                          fixed_density=fixed_density)
+                          fixed_density=fixed_density, ubb_options=ubb_options)
         closure = self.update_rule.collision_rule.closure
         if closure is not None:
             closure.ensure_uploaded()
@@ -192,10 +201,10 @@ class LbKernel:
         return v
 
     def bind(self, pdfs: torch.Tensor, periodic, flags=None, ubb_velocities=None, params=None,
-             stream=None, fixed_density=None) -> BoundSweep:
+             stream=None, fixed_density=None, ubb_options=None) -> BoundSweep:
         check_pdf_tensor(pdfs, self.q, self.update_rule.storage_dtype, "pdfs")
         dims = [s - 2 for s in pdfs.shape[:3]]
-        plan = self.plan(dims, periodic, params or {}, ubb_velocities, fixed_density)
+        plan = self.plan(dims, periodic, params or {}, ubb_velocities, fixed_density, ubb_options)
         return BoundSweep(plan, pdfs.stride(), flags, _stream_handle(stream))
 
     def _parity(self):

@@ -200,9 +200,10 @@ class LatticeBoltzmannStep:
     def _flags(self, kernel):
         if not self._boundary_handling.has_boundaries:
             return None
-        plan = kernel.plan([d for d in self._domain], self.periodicity, self.kernel_params,
-                           self._boundary_handling.ubb_velocities, self._boundary_handling.fixed_density)
-        return self._boundary_handling.flags(plan)
+        bh = self._boundary_handling
+        plan = kernel.plan([d for d in self._domain], self.periodicity, self.kernel_params, bh.ubb_velocities,
+                           bh.fixed_density, bh.ubb_options)
+        return bh.flags(plan)
 
     def _bound(self):
         """The sweep with plan, strides, flags and stream resolved; rebuilt when boundaries,
@@ -214,7 +215,9 @@ class LatticeBoltzmannStep:
             k = self._kernels[0]
             flags = self._flags(k)
             self._bound_sweep = k.bind(self.pdfs, self.periodicity, flags, bh.ubb_velocities, self.kernel_params,
-                                       fixed_density=bh.fixed_density)
+                                       fixed_density=bh.fixed_density, ubb_options=bh.ubb_options)
+            if flags is not None:
+                bh.attach_links(self._bound_sweep.plan)
             self._bound_key = (id(bh._dev), bh._dev is None, tuple(sorted(self.kernel_params.items())),
                                torch.cuda.current_stream().cuda_stream)
         closure = self._kernels[0].update_rule.collision_rule.closure

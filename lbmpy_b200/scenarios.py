@@ -3,7 +3,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .boundaries import UBB, NoSlip, slice_from_direction
+from .boundaries import UBB, FixedDensity, NoSlip, slice_from_direction
+from .geometry import add_pipe_inflow_boundary, add_pipe_walls
 from .lbstep import LatticeBoltzmannStep
 
 
@@ -37,29 +38,42 @@ def create_lid_driven_cavity(domain_size=None, lid_velocity=0.005, lbm_kernel=No
 
 def create_channel(domain_size=None, force=None, pressure_difference=None, u_max=None, diameter_callback=None,
                    duct=False, wall_boundary=None, parallel=False, data_handling=None, **kwargs):
-    """Force-driven channel periodic in x (scenarios.py:105-172).  duct=True: walls on the y and z
-    faces; duct=False: circular pipe of diameter min(ny, nz)."""
+    """Channel along x (scenarios.py:104-172), driven by exactly one of
+    - force: periodic in x, body force (force, 0, 0);
+    - pressure_difference: FixedDensity 1 + pressure_difference on W, FixedDensity 1 on E;
+    - u_max: parabolic pipe inflow on W (add_pipe_inflow_boundary), FixedDensity 1 on E.
+    duct=True: walls on the y and z faces only; duct=False: a pipe of diameter min(ny, nz) (or
+    diameter_callback(x, shape)) inside them."""
     if [bool(p) for p in (force, pressure_difference, u_max)].count(True) != 1:
         raise ValueError("Please specify exactly one of the parameters 'force', 'pressure_difference' or 'u_max'")
-    if not force:
-        raise NotImplementedError("pressure- and velocity-driven channels need FixedDensity / inflow profiles, "
-                                  "which are not built")
     if parallel:
         raise NotImplementedError("use lbmpy_b200.distributed (DistributedLatticeBoltzmannStep) for multi-GPU domains")
     wall_boundary = wall_boundary or NoSlip()
-    kwargs["force"] = (force, 0, 0)
-    step = LatticeBoltzmannStep(domain_size=domain_size, periodicity=(True, False, False),
-                                name="force_driven_channel", **kwargs)
+    domain_size = tuple(int(s) for s in domain_size)
+    periodicity = (True, False, False) if force else (False, False, False)
+    if force:
+        kwargs["force"] = (force, 0, 0)
+        step = LatticeBoltzmannStep(domain_size=domain_size, periodicity=periodicity, name="force_driven_channel",
+                                    **kwargs)
+    elif pressure_difference:
+        step = LatticeBoltzmannStep(domain_size=domain_size, periodicity=periodicity,
+                                    name="pressure_driven_channel", **kwargs)
+        step.boundary_handling.set_boundary(FixedDensity(1.0 + pressure_difference), slice_from_direction("W", 3))
+        step.boundary_handling.set_boundary(FixedDensity(1.0), slice_from_direction("E", 3))
+    else:
+        if duct:
+            raise NotImplementedError("Velocity inflow for duct flows not yet implemented")
+        step = LatticeBoltzmannStep(domain_size=domain_size, periodicity=periodicity,
+                                    name="velocity_driven_channel", **kwargs)
+        diameter = diameter_callback(np.array([0]), domain_size)[0] if diameter_callback else min(domain_size[1:])
+        add_pipe_inflow_boundary(step.boundary_handling, u_max, slice_from_direction("W", 3), flow_direction=0,
+                                 diameter=diameter)
+        step.boundary_handling.set_boundary(FixedDensity(1.0), slice_from_direction("E", 3))
     for d in ("N", "S", "T", "B"):
         step.boundary_handling.set_boundary(wall_boundary, slice_from_direction(d, 3))
+    if duct and diameter_callback is not None:
+        raise ValueError("For duct flows, passing a diameter callback does not make sense.")
     if not duct:
-        if diameter_callback is not None:
-            raise NotImplementedError("diameter callbacks are not built")
-        diameter = min(domain_size[1:])
-        ny, nz = domain_size[1], domain_size[2]
-
-        def outside(x, y, z):
-            return np.sqrt((y - ny / 2) ** 2 + (z - nz / 2) ** 2) >= diameter / 2
-
-        step.boundary_handling.set_boundary(wall_boundary, mask_callback=outside)
+        add_pipe_walls(step.boundary_handling, diameter_callback if diameter_callback else min(domain_size[1:]),
+                       wall_boundary)
     return step

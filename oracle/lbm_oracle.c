@@ -57,6 +57,10 @@ typedef struct {
     float mlp[MLP_NPARAM];    /* sgs == 2: W1[10][32] b1[32] W2[32][32] b2[32] W3[32] b3 scale */
     int discrete_eq;          /* moment based: 1 = discrete Maxwellian (maxwellian_equilibrium.py:64-104,
                                  equilibrium/discrete_hydro_maxwellian.py:9-96), 0 = continuous */
+    int ubb_adapt;            /* UBB: wall velocity shifted by -F / (2 rho_ref) (boundaryconditions.py:790-794) */
+    double ubb_density;       /* UBB: prescribed wall density (compressible), 0: the fluid cell's (:824-830) */
+    const double* ubb_link;   /* UBB: per-link velocities [cell][q][3] (interior cells, x fastest), or NULL */
+    double fd_rho1;           /* density of FixedDensity cells of flag 7 (a second density) */
 } om_method;
 
 typedef struct {
@@ -638,7 +642,7 @@ void om_periodic_sync(const om_method* m, const om_grid* gr, int pattern, int pr
  * 0 fluid, 1 NoSlip, 2 UBB (velocity ubb_u).  f_out / f_in proxies follow
  * advanced_streaming/indexing.py:12-183; NoSlip boundaryconditions.py:128-139,
  * UBB boundaryconditions.py:794-841. */
-/* Flags: 1 NoSlip, 2 UBB (velocity ubb_u), 6 FixedDensity (density fd_rho).
+/* Flags: 1 NoSlip, 2 UBB (velocity ubb_u), 6 / 7 FixedDensity (density fd_rho / m->fd_rho1).
  * FixedDensity (boundaryconditions.py:1044-1099): f_in(inv q) = 2 feq_even_q(rho_w, u) - f_out(q),
  * feq_even the part of the method's equilibrium that is even in u (the mean of directions q and
  * inv q), u from the fluid cell's outgoing populations with the density replaced by rho_w. */
@@ -661,23 +665,32 @@ void om_boundaries(const om_method* m, const om_grid* gr, int pattern, int prev_
             fout = f[gidx(gr, x + ooff[q][0], y + ooff[q][1], z + ooff[q][2]) + oslot[q] * gr->s[3]];
             val = fout;
             if (fl == 2) {
-                double cu = 0.0, rho = 1.0; int k;
-                for (k = 0; k < 3; ++k) cu += m->c[q][k] * ubb_u[k];
+                double cu = 0.0, rho = 1.0, uw[3]; int k;
+                for (k = 0; k < 3; ++k) uw[k] = ubb_u[k];
+                if (m->ubb_link) {
+                    const int64_t c = x + (int64_t)gr->n[0] * (y + (int64_t)gr->n[1] * z);
+                    for (k = 0; k < 3; ++k) uw[k] = m->ubb_link[(c * m->Q + q) * 3 + k];
+                }
                 if (m->compressible) {
                     double s = 0.0;
                     for (k = 0; k < m->Q; ++k)
                         s += f[gidx(gr, x + ooff[k][0], y + ooff[k][1], z + ooff[k][2]) + oslot[k] * gr->s[3]];
                     rho = m->zero_centered ? 1.0 + s : s;
+                    if (m->ubb_density > 0.0) rho = m->ubb_density;
                 }
+                if (m->ubb_adapt)      /* cqc.equilibrium_input_equations_from_init_values(velocity) */
+                    for (k = 0; k < 3; ++k) uw[k] -= m->F[k] / (2.0 * rho);
+                for (k = 0; k < 3; ++k) cu += m->c[q][k] * uw[k];
                 val = fout - 6.0 * m->w[q] * cu * rho;
-            } else if (fl == 6) {
+            } else if (fl == 6 || fl == 7) {
                 double j[3] = {0.0, 0.0, 0.0}, u[3], feq[QMAX]; int k, d;
+                const double rw = fl == 6 ? fd_rho : m->fd_rho1;
                 for (k = 0; k < m->Q; ++k) {
                     const double fk = f[gidx(gr, x + ooff[k][0], y + ooff[k][1], z + ooff[k][2]) + oslot[k] * gr->s[3]];
                     for (d = 0; d < 3; ++d) j[d] += m->c[k][d] * fk;
                 }
-                for (d = 0; d < 3; ++d) u[d] = m->compressible ? j[d] / fd_rho : j[d];
-                om_equilibrium(m, fd_rho, u, feq);
+                for (d = 0; d < 3; ++d) u[d] = m->compressible ? j[d] / rw : j[d];
+                om_equilibrium(m, rw, u, feq);
                 val = feq[q] + feq[iq] - fout;
             }
             f[gidx(gr, x + ioff[iq][0], y + ioff[iq][1], z + ioff[iq][2]) + islot[iq] * gr->s[3]] = val;

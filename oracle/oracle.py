@@ -48,6 +48,10 @@ class OmMethod(ctypes.Structure):
         ("shear_rate", ctypes.c_double),
         ("mlp", ctypes.c_float * MLP_NPARAM),
         ("discrete_eq", ctypes.c_int),
+        ("ubb_adapt", ctypes.c_int),
+        ("ubb_density", ctypes.c_double),
+        ("ubb_link", ctypes.c_void_p),
+        ("fd_rho1", ctypes.c_double),
     ]
 
 
@@ -220,10 +224,20 @@ class Oracle:
         return rho, u
 
     def run(self, f, steps, pattern="pull", parity=0, periodic=(True, True, True), flags=None,
-            ubb_velocity=(0.0, 0.0, 0.0), tmp=None, fixed_density=1.0):
+            ubb_velocity=(0.0, 0.0, 0.0), tmp=None, fixed_density=1.0, ubb_link=None, ubb_adapt=False,
+            ubb_density=None, fixed_density1=1.0):
         """Runs `steps` time steps.  Returns (field holding the result, new parity).  Flags: 1 NoSlip,
-        2 UBB (ubb_velocity), 6 FixedDensity (fixed_density)."""
+        2 UBB (ubb_velocity, or per link ubb_link[x, y, z, q, 3] for the link from interior cell
+        (x, y, z) in direction q; ubb_adapt shifts the wall velocity by -F/(2 rho_ref); ubb_density
+        prescribes the wall density), 6 / 7 FixedDensity (fixed_density / fixed_density1)."""
         g = self._grid(f)
+        link = None
+        if ubb_link is not None:
+            link = np.ascontiguousarray(np.asarray(ubb_link, np.float64).transpose(2, 1, 0, 3, 4))
+        self._m.ubb_link = link.ctypes.data if link is not None else None
+        self._m.ubb_adapt = int(bool(ubb_adapt))
+        self._m.ubb_density = float(ubb_density) if ubb_density else 0.0
+        self._m.fd_rho1 = float(fixed_density1)
         per = (ctypes.c_int * 3)(*[int(p) for p in periodic])
         par = ctypes.c_int(parity)
         ub = np.array(list(ubb_velocity) + [0.0] * (3 - len(ubb_velocity)), np.float64)
@@ -239,10 +253,12 @@ class Oracle:
                               steps, per, fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None
                               else None, self._ptr(ub), ctypes.c_double(fixed_density), self._ptr(f),
                               self._ptr(tmp))
+            self._m.ubb_link = None
             return (tmp if sw else f), par.value
         lib().om_run(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], ctypes.byref(par), steps, per,
                      fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None else None,
                      self._ptr(ub), ctypes.c_double(fixed_density), self._ptr(f), self._ptr(f))
+        self._m.ubb_link = None
         return f, par.value
 
     def periodic_sync(self, f, pattern="pull", prev_parity=0, periodic=(True, True, True)):

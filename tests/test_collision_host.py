@@ -20,7 +20,9 @@ class Physics(ctypes.Structure):
     _fields_ = [("rates", ctypes.c_double * 27), ("force", ctypes.c_double * 3), ("force_model", ctypes.c_int),
                 ("compressible", ctypes.c_int), ("continuous_eq", ctypes.c_int), ("sgs", ctypes.c_int),
                 ("sgs_c18", ctypes.c_double), ("tau0", ctypes.c_double), ("sgs_mask", ctypes.c_uint32),
-                ("galilean", ctypes.c_int), ("ubb", (ctypes.c_double * 3) * 4), ("fixed_density", ctypes.c_double)]
+                ("galilean", ctypes.c_int), ("ubb", (ctypes.c_double * 3) * 4), ("fixed_density", ctypes.c_double),
+                ("fixed_density1", ctypes.c_double), ("ubb_density", ctypes.c_double * 4),
+                ("ubb_link_mask", ctypes.c_uint32), ("ubb_adapt_mask", ctypes.c_uint32)]
 
 
 @pytest.fixture(scope="module")
