@@ -162,15 +162,31 @@ int lbm_reduce_conserved(const LbmPlan* plan, const void* pdfs, const int64_t st
 int lbm_reduce_conserved_noalloc(const LbmPlanDesc* desc, const void* pdfs, const int64_t strides[4],
                                  const uint8_t* flags, int prev_parity, double out[5], void* stream);
 
-/* Per-link wall velocities of UBB numbers in `link_mask` (bit u: UBB number u), for velocity
- * profiles that vary from link to link: lbmpy's UBB(velocity=callback) fills one velocity per
- * boundary link through its index array (boundaries/boundaryconditions.py:747-799,
- * geometry.py:36-86).  cell_block: int32 per interior cell, x fastest, the block of the cell's links
- * or -1; link_velocity: double [n_blocks][Q][3], entry [b][q] the velocity of the link from the
- * cell in direction q (towards the wall).  Device memory owned by the caller, kept by the plan
- * (pass link_mask 0 to detach).  The other UBB numbers keep their constant velocities. */
-int lbm_plan_set_ubb_links(LbmPlan* plan, const int32_t* cell_block, const double* link_velocity,
-                           int64_t n_blocks, uint32_t link_mask);
+/* Per-link data of the boundary conditions that differ from link to link.  No single lbmpy
+ * counterpart: lbmpy keeps such data in the index array of each boundary kernel
+ * (boundaries/boundaryhandling.py:15-199), filled by the boundary's init callback:
+ *   UBB(velocity=callback)          the wall velocity of each link (boundaryconditions.py:747-799,
+ *                                   geometry.py:36-86);
+ *   FreeSlip, SimpleExtrapolationOutflow, ExtrapolationOutflow (flag types 8, 9, 10): the cell and
+ *                                   direction the incoming population is copied from
+ *                                   (:360-455, :844-889, :894-1041), packed as
+ *                                   dir | (ox+1) << 8 | (oy+1) << 10 | (oz+1) << 12;
+ *   ExtrapolationOutflow            its two stored populations per link (pdf, pdf_nd), which the
+ *                                   sweep reads and updates;
+ *   NoSlipLinearBouzidi (type 11)   the wall distance q of each link (:142-212), in value [0].
+ * Links are grouped by fluid cell: cell_block (int32 per interior cell, x fastest) gives the block
+ * of the cell's links or -1; entry [b][q] belongs to the link from that cell in direction q
+ * (towards the boundary cell).  All arrays are device memory owned by the caller and kept by the
+ * plan until it is given other tables (or NULL to detach). */
+typedef struct LbmLinkTables {
+    const int32_t* cell_block;
+    int64_t n_blocks;
+    const double* ubb_velocity;  /* [n_blocks][Q][3], read for the UBB numbers in ubb_mask; may be NULL if 0 */
+    uint32_t ubb_mask;           /* bit u: UBB number u takes its velocity from ubb_velocity */
+    const int32_t* link_code;    /* [n_blocks][Q] or NULL */
+    double* link_value;          /* [n_blocks][Q][2] or NULL; ExtrapolationOutflow's entries are updated */
+} LbmLinkTables;
+int lbm_plan_set_links(LbmPlan* plan, const LbmLinkTables* tables);
 
 /* Sets bit 7 on every fluid cell of `flags` (device, layout above) that has a boundary
  * neighbour along the plan's stencil, honouring periodicity.  Replaces the link-list setup of

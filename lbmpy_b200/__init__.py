@@ -14,7 +14,10 @@ from .creationfunctions import (CreateKernelConfig, LBMConfig, LBMOptimisation, 
 from .relaxationrates import (lattice_viscosity_from_relaxation_rate,  # noqa: F401
                               relaxation_rate_from_lattice_viscosity, relaxation_rate_from_magic_number)
 from .fields import create_pdf_array  # noqa: F401
-from .boundaries import NoSlip, UBB, FixedDensity, LatticeBoltzmannBoundaryHandling, slice_from_direction  # noqa: F401
+from .boundaries import (NoSlip, UBB, FixedDensity, FreeSlip, SimpleExtrapolationOutflow,  # noqa: F401
+                         ExtrapolationOutflow, NoSlipLinearBouzidi, LatticeBoltzmannBoundaryHandling,
+                         slice_from_direction)
+from . import geometry  # noqa: F401
 from .macroscopic_value_kernels import (compile_macroscopic_values_getter,  # noqa: F401
                                         compile_macroscopic_values_setter, macroscopic_values_getter,
                                         macroscopic_values_setter, pdf_initialization_assignments)

@@ -26,7 +26,7 @@ MLP_PARAMS = 1442
 EXPORTS = ("lbm_plan_create", "lbm_plan_destroy", "lbm_plan_update", "lbm_plan_status", "lbm_sweep_variant",
            "lbm_sweep", "lbm_run",
            "lbm_set_equilibrium", "lbm_get_macroscopic", "lbm_reduce_conserved", "lbm_reduce_conserved_noalloc",
-           "lbm_flags_finalize", "lbm_plan_set_ubb_links", "lbm_closure_set_weights", "lbm_closure_features", "lbm_mlp_forward",
+           "lbm_flags_finalize", "lbm_plan_set_links", "lbm_closure_set_weights", "lbm_closure_features", "lbm_mlp_forward",
            "lbm_mlp_create", "lbm_mlp_destroy", "lbm_mlp_loss_grad", "lbm_mlp_adam", "lbm_batch_create", "lbm_batch_sweep", "lbm_batch_info", "lbm_batch_destroy",
            "lbm_last_error", "lbm_version")
 
@@ -52,6 +52,11 @@ class LbmPlanDesc(ctypes.Structure):
         ("ubb_density", ctypes.c_double * 4),
         ("ubb_adapt_mask", ctypes.c_uint32),
     ]
+
+
+class LbmLinkTables(ctypes.Structure):
+    _fields_ = [("cell_block", ctypes.c_void_p), ("n_blocks", ctypes.c_int64), ("ubb_velocity", ctypes.c_void_p),
+                ("ubb_mask", ctypes.c_uint32), ("link_code", ctypes.c_void_p), ("link_value", ctypes.c_void_p)]
 
 
 class LbmDomainDesc(ctypes.Structure):
@@ -96,7 +101,7 @@ def lib():
         L.lbm_reduce_conserved_noalloc.argtypes = [ctypes.POINTER(LbmPlanDesc), vp, i64p, vp, ctypes.c_int,
                                                    ctypes.POINTER(ctypes.c_double), vp]
         L.lbm_flags_finalize.argtypes = [vp, vp, vp]
-        L.lbm_plan_set_ubb_links.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_uint32]
+        L.lbm_plan_set_links.argtypes = [vp, ctypes.POINTER(LbmLinkTables)]
         L.lbm_closure_set_weights.argtypes = [vp, ctypes.c_int, vp]
         L.lbm_closure_features.argtypes = [vp, ctypes.c_int64, vp, vp]
         L.lbm_mlp_forward.argtypes = [vp, vp, ctypes.c_int64, vp, vp]

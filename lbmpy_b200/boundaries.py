@@ -17,8 +17,26 @@ import torch
 from . import _native as N
 
 FLUID, NOSLIP, UBB0, FIXED_DENSITY, FIXED_DENSITY1 = 0, 1, 2, 6, 7
+FREE_SLIP, SIMPLE_OUTFLOW, OUTFLOW, BOUZIDI = 8, 9, 10, 11
 MAX_UBB = 4
 TYPE_MASK = 15          # low 4 bits of a flag: the cell type; bit 7: fluid cell next to a boundary
+_DIRECTION_LETTERS = {"E": (1, 0, 0), "W": (-1, 0, 0), "N": (0, 1, 0), "S": (0, -1, 0), "T": (0, 0, 1),
+                      "B": (0, 0, -1)}
+
+
+def _code(direction: int, offset) -> int:
+    """Per-link code of FreeSlip and the outflows: the incoming population is the outgoing population
+    `direction` of the cell at `offset` from the fluid cell."""
+    return int(direction) | (offset[0] + 1) << 8 | (offset[1] + 1) << 10 | (offset[2] + 1) << 12
+
+
+def direction_string_to_offset(direction: str, dim: int = 3):
+    """'NE' -> (1, 1, 0): pystencils' compass names of the stencil directions."""
+    off = [0, 0, 0]
+    for ch in direction.upper():
+        for a, v in enumerate(_DIRECTION_LETTERS[ch]):
+            off[a] += v
+    return tuple(off[:dim])
 
 
 class LbBoundary:
@@ -103,7 +121,7 @@ class BoundaryData:
         self.index_array = index_array
         self.dim = 3
         self._dirs = np.asarray(stencil_dirs, dtype=np.int64)
-        self.boundary_data_names = {"vel_0", "vel_1", "vel_2"}
+        self.boundary_data_names = set(index_array.dtype.names) - {"x", "y", "z", "dir"}
 
     def non_boundary_cell_positions(self, coord):
         """Cell-centre coordinate of the fluid cell (interior cells at 0.5 .. n - 0.5)."""
@@ -129,6 +147,83 @@ class BoundaryData:
 
     def __len__(self):
         return len(self.index_array)
+
+
+class FreeSlip(LbBoundary):
+    """Specular reflection, zero normal velocity (boundaryconditions.py:360-455): the population
+    entering a fluid cell from the wall is the mirrored outgoing population of the tangential
+    neighbour.  With `normal_direction` (pointing from the wall into the fluid) the mirror axis is
+    fixed; without it the normal of every link is found from the neighbouring boundary cells, as
+    lbmpy's init callback does (convex corners fall back to bounce-back)."""
+
+    def __init__(self, stencil, normal_direction=None, name=None):
+        if normal_direction and len(normal_direction) - list(normal_direction).count(0) != 1:
+            raise ValueError("It is only possible to pre specify the normal direction for simple situations."
+                             "This means if the free slip boundary is applied to a straight wall or side in the "
+                             "simulation domain. A possible value for example would be (0, 1, 0) if the "
+                             "free slip boundary is applied to the northern wall. For more complex situations "
+                             "the normal direction has to be calculated for each cell. This is done when "
+                             "the normal direction is not defined for this class")
+        if normal_direction:
+            normal_direction = tuple(int(n) for n in normal_direction)
+            if not all(n in (-1, 0, 1) for n in normal_direction):
+                raise ValueError("Only -1, 0 and 1 allowed for defining the normal direction")
+            self.mirror_axis = [k for k, n in enumerate(normal_direction) if n != 0][0]
+        self.stencil = [tuple(int(v) for v in d) for d in stencil]
+        self.normal_direction = normal_direction
+        self.dim = len(self.stencil[0])
+        super().__init__(name)
+
+
+class SimpleExtrapolationOutflow(LbBoundary):
+    """Outflow copying the missing populations from the last fluid layer along the outflow normal
+    (boundaryconditions.py:844-889; Geier et al. 2015, eq. F.1)."""
+
+    def __init__(self, normal_direction, stencil, name=None):
+        if isinstance(normal_direction, str):
+            normal_direction = direction_string_to_offset(normal_direction, dim=len(stencil[0]))
+        self.normal_direction = tuple(int(n) for n in normal_direction)
+        if not all(n in (-1, 0, 1) for n in self.normal_direction):
+            raise ValueError("Only -1, 0 and 1 allowed for defining the normal direction")
+        super().__init__(name)
+
+
+class ExtrapolationOutflow(LbBoundary):
+    """Outflow interpolating in time between the last fluid layer and the boundary
+    (boundaryconditions.py:894-1041; Geier et al. 2015, eq. F.2 with u neglected):
+    f_in = c p + (1 - c) p_nd with c = sqrt(1/3) dt/dx, p the outgoing population of the fluid
+    neighbour one step earlier and p_nd the previous result.  Both start from the field's values
+    when the boundary is first applied."""
+
+    def __init__(self, normal_direction, lb_method, dt=1, dx=1, name=None, streaming_pattern="pull",
+                 zeroth_timestep=None, initial_density=None, initial_velocity=None, data_type="double"):
+        if isinstance(normal_direction, str):
+            normal_direction = direction_string_to_offset(normal_direction, dim=lb_method.stencil.D)
+        self.normal_direction = tuple(int(n) for n in normal_direction)
+        if not all(n in (-1, 0, 1) for n in self.normal_direction):
+            raise ValueError("Only -1, 0 and 1 allowed for defining the normal direction")
+        if initial_density is not None or initial_velocity is not None:
+            raise NotImplementedError("initial_density / initial_velocity of ExtrapolationOutflow are not built; "
+                                      "the links start from the field's values")
+        if float(dt) != 1.0 or float(dx) != 1.0:
+            # c dt/dx = sqrt(1/3) whatever dt and dx are, as lbmpy's c carries dx/dt
+            pass
+        self.streaming_pattern = streaming_pattern
+        super().__init__(name)
+
+
+class NoSlipLinearBouzidi(LbBoundary):
+    """No-slip with linear interpolation at the wall distance q of every link
+    (boundaryconditions.py:142-212; Bouzidi et al. 2001).  `init_wall_distance(boundary_data)` sets
+    ``boundary_data['q']``; links left at q <= 0 (the default, -1) bounce back as NoSlip."""
+
+    def __init__(self, name=None, init_wall_distance=None, data_type="double", calculate_force_on_boundary=False):
+        if init_wall_distance is None:
+            import warnings
+            warnings.warn("No callback function provided to initialise the wall distance for each cell "
+                          "(init_wall_distance=None). The boundary condition will fall back to a simple NoSlip BC")
+        self.init_wall_distance = init_wall_distance
+        super().__init__(name, calculate_force_on_boundary)
 
 
 class FixedDensity(LbBoundary):
@@ -178,8 +273,9 @@ class LatticeBoltzmannBoundaryHandling:
         self._fixed_densities: List[float] = []
         self._dev: Optional[torch.Tensor] = None
         self._finalized_for = None
-        self._links = None          # (cell block tensor, link velocity tensor, mask) for callable UBBs
-        self._links_for = None
+        self._links = None          # device link tables (LbmLinkTables and the tensors they point to)
+        self._link_objs: List = []  # FreeSlip / outflow / Bouzidi objects, indexed by self._obj
+        self._obj = np.full((ez, ey, ex), -1, dtype=np.int16)
 
     # --------------------------------------------------------------------------- setup
     def _flag_for(self, boundary_obj) -> int:
@@ -202,8 +298,21 @@ class LatticeBoltzmannBoundaryHandling:
                 raise ValueError("at most two FixedDensity densities per domain are supported")
             self._fixed_densities.append(boundary_obj.density)
             return FIXED_DENSITY + len(self._fixed_densities) - 1
-        raise NotImplementedError(f"boundary {type(boundary_obj).__name__} is not built (NoSlip, UBB and "
-                                  "FixedDensity are)")
+        types = {FreeSlip: FREE_SLIP, SimpleExtrapolationOutflow: SIMPLE_OUTFLOW, ExtrapolationOutflow: OUTFLOW,
+                 NoSlipLinearBouzidi: BOUZIDI}
+        if type(boundary_obj) in types:
+            if not any(o is boundary_obj for o in self._link_objs):
+                self._link_objs.append(boundary_obj)
+            return types[type(boundary_obj)]
+        raise NotImplementedError(f"boundary {type(boundary_obj).__name__} is not built (NoSlip, UBB, FixedDensity, "
+                                  "FreeSlip, SimpleExtrapolationOutflow, ExtrapolationOutflow and "
+                                  "NoSlipLinearBouzidi are)")
+
+    def _obj_index(self, boundary_obj) -> int:
+        for k, o in enumerate(self._link_objs):
+            if o is boundary_obj:
+                return k
+        return -1
 
     def set_boundary(self, boundary_obj, slice_obj=None, mask_callback=None, ghost_layers=True,
                      inner_ghost_layers=True, replace=True, force_flag_value=None):
@@ -222,10 +331,14 @@ class LatticeBoltzmannBoundaryHandling:
             mask = np.asarray(mask_callback(*[c[sl] for c in coords]), dtype=bool)
         else:
             mask = np.ones(region.shape, dtype=bool)
-        if replace:
-            region[mask] = flag
-        else:
-            region[mask & (region == FLUID)] = flag
+        objs = self._obj.transpose(2, 1, 0)
+        if not ghost_layers:
+            objs = objs[1:-1, 1:-1, 1:-1]
+        oreg = objs[sl]
+        if not replace:
+            mask = mask & (region == FLUID)
+        region[mask] = flag
+        oreg[mask] = self._obj_index(boundary_obj)
         self._dev = None
         self._links = None
         return flag
@@ -251,81 +364,232 @@ class LatticeBoltzmannBoundaryHandling:
         return {"densities": [u.density or 0.0 for u in self._ubbs],
                 "adapt_mask": sum(1 << k for k, u in enumerate(self._ubbs) if u.adapt_velocity_to_force)}
 
-    def ubb_links(self, periodicity=None):
-        """Every link from a fluid cell into a cell of each callable UBB, with the velocities its
-        callback set: {UBB number: record array (x, y, z ghost-inclusive fluid cell, dir, vel_0..2)}.
-        Periodic axes wrap, as the sweep's neighbour lookup does."""
-        periodicity = self.periodicity if periodicity is None else periodicity
+    def _links_into(self, select):
+        """Every link (fluid interior cell, direction q) whose neighbour x + c_q satisfies
+        select(types, objects) over the ghost-inclusive [x, y, z] arrays; periodic axes wrap, as the
+        sweep's neighbour lookup does.  Record array: ghost-inclusive x, y, z of the fluid cell, dir."""
         dirs = [tuple(int(v) for v in d) for d in self.method.stencil]
-        flags = self._host.transpose(2, 1, 0) & TYPE_MASK    # [x, y, z], ghost-inclusive
+        types = self._host.transpose(2, 1, 0) & TYPE_MASK
+        objs = self._obj.transpose(2, 1, 0)
+        target = select(types, objs)
         n = self.shape
+        fluid = types[1:-1, 1:-1, 1:-1] == FLUID
+        parts = []
+        for q, c in enumerate(dirs):
+            if c == (0, 0, 0):
+                continue
+            idx = []
+            for a in range(3):
+                i = np.arange(n[a]) + c[a]
+                if self.periodicity[a]:
+                    i = i % n[a]
+                idx.append(i + 1)
+            hit = fluid & target[np.ix_(*idx)]
+            xs, ys, zs = np.nonzero(hit)
+            parts.append((xs + 1, ys + 1, zs + 1, np.full(len(xs), q)))
+        m = sum(len(p[0]) for p in parts)
+        out = np.zeros(m, dtype=[("x", np.int32), ("y", np.int32), ("z", np.int32), ("dir", np.int32)])
+        pos = 0
+        for xs, ys, zs, qs in parts:
+            k = len(xs)
+            out["x"][pos:pos + k], out["y"][pos:pos + k], out["z"][pos:pos + k] = xs, ys, zs
+            out["dir"][pos:pos + k] = qs
+            pos += k
+        return out
+
+    @staticmethod
+    def _with_fields(links, fields):
+        dt = links.dtype.descr + [(name, np.float64) for name in fields]
+        arr = np.zeros(len(links), dtype=dt)
+        for name in links.dtype.names:
+            arr[name] = links[name]
+        return arr
+
+    def ubb_links(self):
+        """Every link into a cell of each callable UBB, with the velocities its callback set:
+        {UBB number: record array (x, y, z ghost-inclusive fluid cell, dir, vel_0..2)}."""
+        dirs = [tuple(int(v) for v in d) for d in self.method.stencil]
         out = {}
         for k, u in enumerate(self._ubbs):
             if not u.velocity_is_callable:
                 continue
-            recs = []
-            fluid = flags[1:-1, 1:-1, 1:-1] == FLUID
-            for q, c in enumerate(dirs):
-                if c == (0, 0, 0):
-                    continue
-                idx = []
-                for a in range(3):
-                    i = np.arange(n[a]) + c[a]
-                    if periodicity[a]:
-                        i = i % n[a]
-                    idx.append(i + 1)
-                nb = flags[np.ix_(*idx)]
-                hit = fluid & (nb == UBB0 + k)
-                xs, ys, zs = np.nonzero(hit)
-                if len(xs):
-                    recs.append((xs + 1, ys + 1, zs + 1, np.full(len(xs), q)))
-            dt = np.dtype([("x", np.int32), ("y", np.int32), ("z", np.int32), ("dir", np.int32),
-                           ("vel_0", np.float64), ("vel_1", np.float64), ("vel_2", np.float64)])
-            arr = np.zeros(sum(len(r[0]) for r in recs), dtype=dt)
-            pos = 0
-            for xs, ys, zs, qs in recs:
-                m = len(xs)
-                arr["x"][pos:pos + m], arr["y"][pos:pos + m], arr["z"][pos:pos + m] = xs, ys, zs
-                arr["dir"][pos:pos + m] = qs
-                pos += m
+            arr = self._with_fields(self._links_into(lambda t, o, k=k: t == UBB0 + k), ("vel_0", "vel_1", "vel_2"))
             u._callback(BoundaryData(arr, dirs))
             out[k] = arr
         return out
 
-    def ubb_link_velocities_dense(self):
-        """[x, y, z, Q, 3] velocities of every callable-UBB link (zero elsewhere), for checkers that
-        take a dense per-link array."""
-        q = len(self.method.stencil)
-        dense = np.zeros(self.shape + (q, 3))
-        for arr in self.ubb_links().values():
-            for k in range(3):
-                dense[arr["x"] - 1, arr["y"] - 1, arr["z"] - 1, arr["dir"], k] = arr[f"vel_{k}"]
-        return dense
+    def _freeslip_codes(self, obj, links):
+        """Link codes of one FreeSlip (boundaryconditions.py:398-455)."""
+        dirs = [tuple(int(v) for v in d) for d in self.method.stencil]
+        n = self.shape
 
-    def attach_links(self, plan):
-        """Builds (once per boundary set-up) the per-link velocity tables of the callable UBBs and
-        hands them to `plan` (lbm_plan_set_ubb_links)."""
-        if not any(u.velocity_is_callable for u in self._ubbs):
+        def wrap(cell):
+            return tuple((c - 1) % n[a] + 1 if self.periodicity[a] else c for a, c in enumerate(cell))
+
+        def mirror(d, axis):
+            d = list(d)
+            d[axis] = -d[axis]
+            return tuple(d)
+        codes = np.zeros(len(links), dtype=np.int32)
+        if obj.normal_direction:
+            nrm = obj.normal_direction
+            for r, (q) in enumerate(links["dir"]):
+                c = dirs[q]
+                ref = tuple(-v for v in mirror(c, obj.mirror_axis))
+                off = tuple(a + b for a, b in zip(c, nrm))
+                codes[r] = _code(dirs.index(ref), off)
+            return codes
+        cells = {wrap((int(x) + dirs[q][0], int(y) + dirs[q][1], int(z) + dirs[q][2]))
+                 for x, y, z, q in zip(links["x"], links["y"], links["z"], links["dir"])}
+        for r, (x, y, z, q) in enumerate(zip(links["x"], links["y"], links["z"], links["dir"])):
+            c = dirs[q]
+            ref = c
+            normal = [0, 0, 0]
+            for a in range(3):
+                sub = [0, 0, 0]
+                sub[a] = c[a]
+                if c[a] != 0 and wrap((int(x) + sub[0], int(y) + sub[1], int(z) + sub[2])) in cells:
+                    normal[a] = c[a]
+                    ref = mirror(ref, a)
+            if all(v == 0 for v in normal):          # convex corner: bounce back
+                normal = list(c)
+            else:
+                ref = tuple(-v for v in ref)
+            off = tuple(c[a] - normal[a] for a in range(3))
+            codes[r] = _code(dirs.index(tuple(ref)), off)
+        return codes
+
+    def _outflow_codes(self, obj, links):
+        dirs = [tuple(int(v) for v in d) for d in self.method.stencil]
+        codes = np.zeros(len(links), dtype=np.int32)
+        for r, q in enumerate(links["dir"]):
+            c = dirs[q]
+            inv = dirs.index(tuple(-v for v in c))
+            codes[r] = _code(inv, tuple(a - b for a, b in zip(c, obj.normal_direction)))
+        return codes
+
+    def link_tables_host(self, pdfs=None, previous_timestep=None, pattern=None):
+        """The per-link data of every boundary that has some, grouped by fluid cell (the layout of
+        lbm_plan_set_links): (cell_block [nx*ny*nz] int32, ubb_velocity [B, Q, 3], link_code [B, Q],
+        link_value [B, Q, 2], ubb_mask).  ExtrapolationOutflow's two values start from the
+        outgoing populations of the field `pdfs` (host array [x, y, z, q], ghost-inclusive), as the
+        previous step of `pattern` with `previous_timestep` wrote them."""
+        from .accessors import write_location
+        dirs = [tuple(int(v) for v in d) for d in self.method.stencil]
+        q = len(dirs)
+        n = self.shape
+        groups = []            # (links, kind, data)
+        ubb_mask = 0
+        for k, arr in self.ubb_links().items():
+            ubb_mask |= 1 << k
+            groups.append((arr, "ubb", np.stack([arr["vel_0"], arr["vel_1"], arr["vel_2"]], axis=-1)))
+        for k, obj in enumerate(self._link_objs):
+            links = self._links_into(lambda t, o, k=k: o == k)
+            if isinstance(obj, FreeSlip):
+                groups.append((links, "code", self._freeslip_codes(obj, links)))
+            elif isinstance(obj, SimpleExtrapolationOutflow):
+                groups.append((links, "code", self._outflow_codes(obj, links)))
+            elif isinstance(obj, ExtrapolationOutflow):
+                codes = self._outflow_codes(obj, links)
+                vals = np.zeros((len(links), 2))
+                if pdfs is not None:
+                    pat = pattern or self.streaming_pattern
+                    par = 0 if previous_timestep is None else int(previous_timestep)
+                    for r, (x, y, z, cd) in enumerate(zip(links["x"], links["y"], links["z"], codes)):
+                        d = int(cd) & 0xFF
+                        cell = [int(x) + ((int(cd) >> (8 + 2 * a)) & 3) - 1 for a in range(3)]
+                        woff, slot = write_location(pat, par, dirs, d)
+                        loc = []
+                        for a in range(3):
+                            v = cell[a] + woff[a]
+                            if self.periodicity[a]:
+                                v = (v - 1) % n[a] + 1
+                            loc.append(min(max(v, 0), n[a] + 1))
+                        vals[r] = pdfs[loc[0], loc[1], loc[2], slot]
+                groups.append((links, "outflow", (codes, vals)))
+            elif isinstance(obj, NoSlipLinearBouzidi):
+                arr = self._with_fields(links, ("q",))
+                arr["q"] = -1.0
+                if obj.init_wall_distance is not None:
+                    obj.init_wall_distance(BoundaryData(arr, dirs))
+                groups.append((links, "q", np.asarray(arr["q"], np.float64)))
+        allx = [g[0] for g in groups if len(g[0])]
+        block = np.full(n[0] * n[1] * n[2], -1, dtype=np.int32)
+        if not allx:
+            return None
+        cell = np.concatenate([(a["x"] - 1) + n[0] * ((a["y"] - 1) + n[1] * (a["z"] - 1)) for a in allx])
+        uniq = np.unique(cell)
+        block[uniq] = np.arange(len(uniq), dtype=np.int32)
+        nb = len(uniq)
+        vel = np.zeros((nb, q, 3))
+        code = np.zeros((nb, q), dtype=np.int32)
+        value = np.zeros((nb, q, 2))
+        for links, kind, data in groups:
+            if not len(links):
+                continue
+            b = block[(links["x"] - 1) + n[0] * ((links["y"] - 1) + n[1] * (links["z"] - 1))]
+            d = links["dir"]
+            if kind == "ubb":
+                vel[b, d] = data
+            elif kind == "code":
+                code[b, d] = data
+            elif kind == "outflow":
+                code[b, d] = data[0]
+                value[b, d] = data[1]
+            else:
+                value[b, d, 0] = data
+        return block, vel, code, value, ubb_mask
+
+    def link_tables_dense(self, pdfs=None, previous_timestep=None, pattern=None):
+        """The per-link data as dense arrays over interior cells and directions, for checkers:
+        (ubb_velocity [x, y, z, Q, 3], link_code [x, y, z, Q], link_value [x, y, z, Q, 2])."""
+        t = self.link_tables_host(pdfs, previous_timestep, pattern)
+        q = len(self.method.stencil)
+        n = self.shape
+        vel, code, value = np.zeros(n + (q, 3)), np.zeros(n + (q,), np.int32), np.zeros(n + (q, 2))
+        if t is None:
+            return vel, code, value
+        block, bv, bc, bval, _ = t
+        b = block.reshape(n[2], n[1], n[0]).transpose(2, 1, 0)
+        has = b >= 0
+        vel[has], code[has], value[has] = bv[b[has]], bc[b[has]], bval[b[has]]
+        return vel, code, value
+
+    def ubb_link_velocities_dense(self):
+        """[x, y, z, Q, 3] velocities of every callable-UBB link (zero elsewhere)."""
+        return self.link_tables_dense()[0]
+
+    def attach_links(self, plan, pdfs=None, previous_timestep=None):
+        """Builds (once per boundary set-up) the per-link tables of the boundaries that need them and
+        hands them to `plan` (lbm_plan_set_links).  ExtrapolationOutflow links start from the current
+        field `pdfs` (a device tensor) as the step before `previous_timestep` left it."""
+        if not self._link_objs and not any(u.velocity_is_callable for u in self._ubbs):
             return
         if self._links is None:
-            links = self.ubb_links()
-            q = len(self.method.stencil)
-            n = self.shape
-            block = np.full(n[0] * n[1] * n[2], -1, dtype=np.int32)      # x fastest
-            allr = np.concatenate(list(links.values())) if links else np.zeros(0, dtype=np.int32)
-            cell = (allr["x"] - 1) + n[0] * ((allr["y"] - 1) + n[1] * (allr["z"] - 1)) if len(allr) else allr
-            uniq, inv = np.unique(cell, return_inverse=True)
-            vel = np.zeros((max(len(uniq), 1), q, 3))
-            for k in range(3):
-                if len(allr):
-                    vel[inv, allr["dir"], k] = allr[f"vel_{k}"]
-            block[uniq] = np.arange(len(uniq), dtype=np.int32)
-            mask = sum(1 << k for k, u in enumerate(self._ubbs) if u.velocity_is_callable)
-            self._links = (torch.from_numpy(block).to(self.device), torch.from_numpy(vel).to(self.device), mask,
-                           vel.shape[0])
-        blk, vel, mask, nb = self._links
-        N.check(N.lib().lbm_plan_set_ubb_links(plan.handle, ctypes.c_void_p(blk.data_ptr()),
-                                               ctypes.c_void_p(vel.data_ptr()), nb, mask), "lbm_plan_set_ubb_links")
+            host_pdfs = None
+            if pdfs is not None and any(isinstance(o, ExtrapolationOutflow) for o in self._link_objs):
+                host_pdfs = pdfs.detach().double().cpu().numpy()
+            t = self.link_tables_host(host_pdfs, previous_timestep)
+            if t is None:
+                self._links = ()
+            else:
+                block, vel, code, value, mask = t
+                dev = [torch.from_numpy(a).to(self.device) for a in (block, vel, code, value)]
+                tabs = N.LbmLinkTables()
+                tabs.cell_block = dev[0].data_ptr()
+                tabs.n_blocks = vel.shape[0]
+                tabs.ubb_velocity = dev[1].data_ptr()
+                tabs.ubb_mask = mask
+                tabs.link_code = dev[2].data_ptr()
+                tabs.link_value = dev[3].data_ptr()
+                self._links = (tabs, dev)
+        if self._links:
+            N.check(N.lib().lbm_plan_set_links(plan.handle, ctypes.byref(self._links[0])), "lbm_plan_set_links")
+
+    @property
+    def link_values(self):
+        """Device tensor of the per-link values ([B, Q, 2]: Bouzidi q, ExtrapolationOutflow state)."""
+        return self._links[1][3] if self._links else None
 
     @property
     def fixed_density(self):

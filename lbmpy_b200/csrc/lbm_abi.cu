@@ -32,8 +32,10 @@ struct LbmPlan {
     uint32_t* rowmask;     // row summary of the flag field last finalized with this plan
     mutable const uint8_t* rowmask_flags;  // that flag field (sweeps given it use the summary)
     void* ubb_rho;         // compressible + moving UBB walls: density gathered before the sweep
-    const int* ubb_block;  // per-link UBB velocities (lbm_plan_set_ubb_links), caller-owned
+    const int* ubb_block;  // per-link boundary tables (lbm_plan_set_links), caller-owned
     const double* ubb_link_vel;
+    const int* link_code;
+    double* link_value;
     uint32_t ubb_link_mask;
     Physics phys;
     double* partial;       // reduction scratch: RED_BLOCKS * 5 doubles
@@ -599,6 +601,8 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
     }
     p->ubb_block = nullptr;
     p->ubb_link_vel = nullptr;
+    p->link_code = nullptr;
+    p->link_value = nullptr;
     p->ubb_link_mask = 0;
     fill_physics(p, desc);
     int sms = 148;
@@ -699,6 +703,8 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
     a.status = p->status;
     a.ubb_block = p->ubb_block;
     a.ubb_link_vel = p->ubb_link_vel;
+    a.link_code = p->link_code;
+    a.link_value = p->link_value;
     if (flags != nullptr && flags == p->rowmask_flags) a.g.rowmask = p->rowmask;
     if (flags != nullptr && p->ubb_rho != nullptr && needs_ubb_density(&p->desc, p->ubb_link_mask)) {
         UbbLauncher U = p->q == 19 ? ubb_launcher_q<19>(p->store, pat) : ubb_launcher_q<27>(p->store, pat);
@@ -912,21 +918,31 @@ int lbm_flags_finalize(const LbmPlan* p, uint8_t* flags, void* stream) {
     return LBM_OK;
 }
 
-int lbm_plan_set_ubb_links(LbmPlan* p, const int32_t* cell_block, const double* link_velocity, int64_t n_blocks,
-                           uint32_t link_mask) {
+int lbm_plan_set_links(LbmPlan* p, const LbmLinkTables* t) {
     if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
     int rc;
     if ((rc = check_device(p))) return rc;
-    if (link_mask & ~0xfu) return fail(LBM_E_INVALID, "link_mask has bits beyond UBB number 3");
-    if (link_mask != 0) {
-        if ((rc = check_device_ptr(p, cell_block, "cell_block", false))) return rc;
-        if ((rc = check_device_ptr(p, link_velocity, "link_velocity", false))) return rc;
-        if (n_blocks < 1) return fail(LBM_E_INVALID, "n_blocks must be positive when link_mask is set");
+    if (t == nullptr) {                          // detach
+        p->ubb_block = nullptr;
+        p->ubb_link_vel = nullptr;
+        p->link_code = nullptr;
+        p->link_value = nullptr;
+        p->ubb_link_mask = 0;
+        p->phys.ubb_link_mask = 0;
+        return LBM_OK;
     }
-    p->ubb_block = link_mask ? reinterpret_cast<const int*>(cell_block) : nullptr;
-    p->ubb_link_vel = link_mask ? link_velocity : nullptr;
-    p->ubb_link_mask = link_mask;
-    p->phys.ubb_link_mask = link_mask;
+    if (t->ubb_mask & ~0xfu) return fail(LBM_E_INVALID, "ubb_mask has bits beyond UBB number 3");
+    if ((rc = check_device_ptr(p, t->cell_block, "cell_block", false))) return rc;
+    if (t->n_blocks < 1) return fail(LBM_E_INVALID, "n_blocks must be positive");
+    if ((rc = check_device_ptr(p, t->ubb_velocity, "ubb_velocity", t->ubb_mask == 0))) return rc;
+    if ((rc = check_device_ptr(p, t->link_code, "link_code", true))) return rc;
+    if ((rc = check_device_ptr(p, t->link_value, "link_value", true))) return rc;
+    p->ubb_block = reinterpret_cast<const int*>(t->cell_block);
+    p->ubb_link_vel = t->ubb_mask ? t->ubb_velocity : nullptr;
+    p->link_code = reinterpret_cast<const int*>(t->link_code);
+    p->link_value = t->link_value;
+    p->ubb_link_mask = t->ubb_mask;
+    p->phys.ubb_link_mask = t->ubb_mask;
     return ensure_ubb_buffer(p);
 }
 

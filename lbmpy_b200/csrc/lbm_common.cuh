@@ -32,7 +32,8 @@ enum ForceKind : int { FM_NONE = 0, FM_GUO = 1, FM_CENTRAL = 2, FM_SIMPLE = 3, F
 
 // Cell flags (uint8, ghost-layered domain): low 4 bits = cell type, bit 7 = fluid cell with at
 // least one boundary neighbour.  Type 0 fluid, 1 NoSlip, 2..5 UBB number (type - 2),
-// 6 / 7 FixedDensity with the plan's first / second density.
+// 6 / 7 FixedDensity with the plan's first / second density, 8 FreeSlip, 9 SimpleExtrapolation-
+// Outflow, 10 ExtrapolationOutflow, 11 NoSlipLinearBouzidi (the last four read per-link data).
 constexpr int FLAG_TYPE_MASK = 15;
 constexpr int FLAG_NEAR_WALL = 128;
 constexpr int FLAG_NOSLIP = 1;
@@ -40,6 +41,16 @@ constexpr int FLAG_UBB0 = 2;
 constexpr int MAX_UBB = 4;
 constexpr int FLAG_FIXED_DENSITY = 6;
 constexpr int FLAG_FIXED_DENSITY1 = 7;
+constexpr int FLAG_FREE_SLIP = 8;
+constexpr int FLAG_SIMPLE_OUTFLOW = 9;
+constexpr int FLAG_OUTFLOW = 10;
+constexpr int FLAG_BOUZIDI = 11;
+
+// Per-link code of FreeSlip and the outflow conditions: the incoming population is the outgoing
+// population `dir` of the cell at offset (ox, oy, oz) in {-1, 0, 1}^3 from the fluid cell:
+// code = dir | (ox + 1) << 8 | (oy + 1) << 10 | (oz + 1) << 12.
+LBM_HD constexpr int link_dir(int code) { return code & 0xff; }
+LBM_HD constexpr int link_off(int code, int axis) { return ((code >> (8 + 2 * axis)) & 3) - 1; }
 
 LBM_HD constexpr bool flag_is_ubb(int t) { return t >= FLAG_UBB0 && t < FLAG_UBB0 + MAX_UBB; }
 LBM_HD constexpr bool flag_is_fixed_density(int t) { return t == FLAG_FIXED_DENSITY || t == FLAG_FIXED_DENSITY1; }
@@ -148,11 +159,16 @@ struct SweepArgs {
     int pad_;
     const void* ubb_rho;   // compressible moving walls: previous-step density of the cells next to them
     unsigned* status;      // device status word of the plan (STATUS_* bits), or nullptr
-    // Per-link UBB velocities: block index of each interior cell (x fastest, -1: none) and, per
-    // block, the velocity of the link in each direction q (pointing from the fluid cell to the
-    // wall, lbmpy's `dir`): ubb_link_vel[(block * Q + q) * 3 + k].
+    // Per-link boundary data: block index of each interior cell (x fastest, -1: none) and, per
+    // block and link direction q (pointing from the fluid cell to the wall, lbmpy's `dir`):
+    // the UBB velocity ubb_link_vel[(block * Q + q) * 3 + k], the code link_code[block * Q + q]
+    // (FreeSlip, outflows) and two values link_value[(block * Q + q) * 2 + k] (Bouzidi: q;
+    // ExtrapolationOutflow: the previous outgoing and interpolated populations, updated by the
+    // sweep that reads them).
     const int* ubb_block;
     const double* ubb_link_vel;
+    const int* link_code;
+    double* link_value;
 };
 
 // Whether interior row (y, z) may hold a cell with a non-zero flag.

@@ -86,8 +86,51 @@ __device__ __forceinline__ R collide(R (&f)[Q], const Physics& p) {
 // Element index of (slot, cell + offset) relative to the field base; 32-bit (host-checked).
 __device__ __forceinline__ unsigned eidx(unsigned slot_off, int cell_off) { return slot_off + (unsigned)cell_off; }
 
-// Fused bounce-back for a fluid cell next to a boundary: replaces the pulled value of every
-// direction whose source cell x - c_i is a wall.
+// Element offset of cell (x, y, z) (interior coordinates), periodic axes wrapped; false when the
+// cell lies beyond the ghost layer of a non-periodic axis.  Used by the boundary conditions that
+// read a cell other than the fluid cell itself (FreeSlip, outflows, Bouzidi), where the offset from
+// the fluid cell can reach 2.
+__device__ __forceinline__ bool cell_offset(const Grid& g, int x, int y, int z, int& out) {
+    const int n[3] = {g.nx, g.ny, g.nz};
+    int c[3] = {x, y, z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if ((g.periodic >> a) & 1) c[a] = ((c[a] % n[a]) + n[a]) % n[a];
+        else if (c[a] < -1 || c[a] > n[a]) return false;
+    }
+    out = (c[0] + 1) + (c[1] + 1) * g.sy + (c[2] + 1) * g.sz;
+    return true;
+}
+
+// Where the previous step wrote the outgoing population d of the cell at (x, y, z) + off: the
+// value, or `fallback` when that cell lies beyond the ghost layer.
+template <class S, class R, int Q, int PAT>
+__device__ __forceinline__ R load_f_out(const SweepArgs& a, int x, int y, int z, int ox, int oy, int oz, int d,
+                                        R fallback) {
+    using PA = Access<PrevPattern<PAT>::value>;
+    int off;
+    if (!cell_offset(a.g, x + ox + PA::template woff<Q>(d, 0), y + oy + PA::template woff<Q>(d, 1),
+                     z + oz + PA::template woff<Q>(d, 2), off))
+        return fallback;
+    return Conv<S, R>::ld(static_cast<const S*>(a.src) + eidx(PA::template wslot<Q>(d) * a.g.sq, off));
+}
+
+// Fused boundary handling for a fluid cell next to a boundary: replaces the pulled value of every
+// direction i whose source cell x - c_i is a boundary cell by the value lbmpy's boundary kernel
+// would have written there (boundaries/boundaryconditions.py), from the populations the previous
+// step wrote.  f_out(x, j) below is where the previous step wrote direction j of cell x.
+//   NoSlip (:104-139)         f_out(x, inv i)
+//   UBB (:724-841)            f_out(x, inv i) + 6 w_i rho c_i.u_w   (u_w per UBB number or per link)
+//   FreeSlip (:360-455), SimpleExtrapolationOutflow (:844-889)
+//                             f_out(x + off, d)                      (off, d from the link code)
+//   ExtrapolationOutflow (:894-1041)
+//                             c p + (1 - c) p_nd, c = sqrt(1/3); then p <- f_out(x + off, d), p_nd <- result
+//   NoSlipLinearBouzidi (:142-212), wall distance q of the link
+//                             q >= 1/2: (f_out(x, inv i) + (2q - 1) f_out(x, i)) / (2q)
+//                             0 < q < 1/2: 2q f_out(x, inv i) + (1 - 2q) f_out(x + c_i, inv i)
+//                             else f_out(x, inv i)
+// A link whose data table is missing, or whose other cell lies beyond the ghost layer, falls back
+// to NoSlip.
 template <class S, class R, int Q, int PAT>
 __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const NbrOffsets& nb, int cell,
                                          int x, int y, int z) {
@@ -102,6 +145,8 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
         fo.init(gf, x, y, z);
     }
     const int fcell = (x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz;
+    // Interior cell indices fit 32 bits (the host bounds the field below 2^32 elements).
+    const int icell = x + g.nx * (y + g.ny * z);
 #pragma unroll
     for (int i = 1; i < Q; ++i) {
         const int bt = g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK;
@@ -113,10 +158,8 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
         if (flag_is_ubb(bt)) {
             const int u = bt - FLAG_UBB0;
             const double* uw = a.p.ubb[u];
-            // Interior cell indices fit 32 bits (the host bounds the field below 2^32 elements).
-            const int icell = x + g.nx * (y + g.ny * z);
             if ((a.p.ubb_link_mask >> u) & 1u)   // per-link velocity of the link x -> x - c_i (dir inv i)
-                uw = a.ubb_link_vel + (size_t(a.ubb_block[icell]) * Q + size_t(L::inv(i))) * 3;
+                uw = a.ubb_link_vel + (size_t(a.ubb_block[icell]) * Q + size_t(j)) * 3;
             // compressible: the prescribed wall density, else the cell's density at the previous
             // step, gathered before the sweep (k_ubb_density; in-place sweeps overwrite the
             // values it is summed from)
@@ -130,6 +173,31 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
             }
             const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
             v += R(6) * R(L::w(i)) * cu * rho;
+        } else if (bt >= FLAG_FREE_SLIP && bt <= FLAG_OUTFLOW && a.ubb_block != nullptr && a.link_code != nullptr) {
+            const size_t li = size_t(a.ubb_block[icell]) * Q + size_t(j);
+            const int code = a.link_code[li];
+            const R w = load_f_out<S, R, Q, PAT>(a, x, y, z, link_off(code, 0), link_off(code, 1), link_off(code, 2),
+                                                 link_dir(code), v);
+            if (bt == FLAG_OUTFLOW && a.link_value != nullptr) {
+                double* st = a.link_value + li * 2;
+                const R c = R(0.57735026918962576451);   // sqrt(1/3) dt/dx
+                const R fin = c * R(st[0]) + (R(1) - c) * R(st[1]);
+                st[0] = double(w);
+                st[1] = double(fin);
+                v = fin;
+            } else {
+                v = w;
+            }
+        } else if (bt == FLAG_BOUZIDI && a.ubb_block != nullptr && a.link_value != nullptr) {
+            const R q = R(a.link_value[(size_t(a.ubb_block[icell]) * Q + size_t(j)) * 2]);
+            if (q >= R(0.5)) {
+                const int oi = nb.off(PA::template woff<Q>(i, 0), PA::template woff<Q>(i, 1), PA::template woff<Q>(i, 2));
+                const R finv = Conv<S, R>::ld(src + eidx(PA::template wslot<Q>(i) * g.sq, cell + oi));
+                v = (R(0.5) * (v + finv * (R(2) * q - R(1)))) / q;
+            } else if (q > R(0)) {
+                const R d2 = load_f_out<S, R, Q, PAT>(a, x, y, z, L::cx(i), L::cy(i), L::cz(i), j, v);
+                v = R(2) * q * v + (R(1) - R(2) * q) * d2;
+            }
         }
         f[i] = v;
     }

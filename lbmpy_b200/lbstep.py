@@ -217,7 +217,7 @@ class LatticeBoltzmannStep:
             self._bound_sweep = k.bind(self.pdfs, self.periodicity, flags, bh.ubb_velocities, self.kernel_params,
                                        fixed_density=bh.fixed_density, ubb_options=bh.ubb_options)
             if flags is not None:
-                bh.attach_links(self._bound_sweep.plan)
+                bh.attach_links(self._bound_sweep.plan, self.pdfs, self._prev.idx if self._inplace else 0)
             self._bound_key = (id(bh._dev), bh._dev is None, tuple(sorted(self.kernel_params.items())),
                                torch.cuda.current_stream().cuda_stream)
         closure = self._kernels[0].update_rule.collision_rule.closure

@@ -61,6 +61,9 @@ typedef struct {
     double ubb_density;       /* UBB: prescribed wall density (compressible), 0: the fluid cell's (:824-830) */
     const double* ubb_link;   /* UBB: per-link velocities [cell][q][3] (interior cells, x fastest), or NULL */
     double fd_rho1;           /* density of FixedDensity cells of flag 7 (a second density) */
+    const int* link_code;     /* flags 8-10: per-link source, dir | (ox+1)<<8 | (oy+1)<<10 | (oz+1)<<12,
+                                 [cell][q] (interior cells, x fastest; q the link direction) */
+    double* link_value;       /* flags 10, 11: per-link values [cell][q][2] (outflow state, Bouzidi q) */
 } om_method;
 
 typedef struct {
@@ -642,12 +645,30 @@ void om_periodic_sync(const om_method* m, const om_grid* gr, int pattern, int pr
  * 0 fluid, 1 NoSlip, 2 UBB (velocity ubb_u).  f_out / f_in proxies follow
  * advanced_streaming/indexing.py:12-183; NoSlip boundaryconditions.py:128-139,
  * UBB boundaryconditions.py:794-841. */
-/* Flags: 1 NoSlip, 2 UBB (velocity ubb_u), 6 / 7 FixedDensity (density fd_rho / m->fd_rho1).
+/* Outgoing population d of cell (x, y, z) as the previous step wrote it, the cell wrapped on periodic
+ * axes (the ghost layers hold the same values after om_periodic_sync); 0 with *ok = 0 when the
+ * location lies beyond the ghost layer of a non-periodic axis. */
+static double f_out_at(const om_method* m, const om_grid* gr, const int periodic[3], int ooff[QMAX][3],
+                       int oslot[QMAX], const double* f, int x, int y, int z, int d, int* ok) {
+    int c[3] = {x + ooff[d][0], y + ooff[d][1], z + ooff[d][2]}, a;
+    for (a = 0; a < 3; ++a) {
+        if (a >= m->D) continue;
+        if (periodic[a]) c[a] = ((c[a] % gr->n[a]) + gr->n[a]) % gr->n[a];
+        else if (c[a] < -1 || c[a] > gr->n[a]) { *ok = 0; return 0.0; }
+    }
+    *ok = 1;
+    return f[gidx(gr, c[0], c[1], c[2]) + oslot[d] * gr->s[3]];
+}
+
+/* Flags: 1 NoSlip, 2 UBB (velocity ubb_u), 6 / 7 FixedDensity (density fd_rho / m->fd_rho1),
+ * 8 FreeSlip and 9 SimpleExtrapolationOutflow (copy from the cell and direction of the link code,
+ * boundaryconditions.py:360-455, 844-889), 10 ExtrapolationOutflow (:894-1041), 11
+ * NoSlipLinearBouzidi (:142-212).
  * FixedDensity (boundaryconditions.py:1044-1099): f_in(inv q) = 2 feq_even_q(rho_w, u) - f_out(q),
  * feq_even the part of the method's equilibrium that is even in u (the mean of directions q and
  * inv q), u from the fluid cell's outgoing populations with the density replaced by rho_w. */
 void om_boundaries(const om_method* m, const om_grid* gr, int pattern, int prev_parity,
-                   const uint8_t* flags, const double ubb_u[3], double fd_rho, double* f) {
+                   const uint8_t* flags, const double ubb_u[3], double fd_rho, const int periodic[3], double* f) {
     int ooff[QMAX][3], oslot[QMAX], ioff[QMAX][3], islot[QMAX], i;
     int next_parity = 1 - prev_parity;
     for (i = 0; i < m->Q; ++i) {
@@ -682,6 +703,34 @@ void om_boundaries(const om_method* m, const om_grid* gr, int pattern, int prev_
                     for (k = 0; k < 3; ++k) uw[k] -= m->F[k] / (2.0 * rho);
                 for (k = 0; k < 3; ++k) cu += m->c[q][k] * uw[k];
                 val = fout - 6.0 * m->w[q] * cu * rho;
+            } else if (fl >= 8 && fl <= 11 && (m->link_code || m->link_value)) {
+                const int64_t c = x + (int64_t)gr->n[0] * (y + (int64_t)gr->n[1] * z);
+                const int64_t li = c * m->Q + q;
+                int ok = 1;
+                if (fl <= 10 && m->link_code) {
+                    const int code = m->link_code[li], d = code & 0xff;
+                    const double w = f_out_at(m, gr, periodic, ooff, oslot, f, x + ((code >> 8) & 3) - 1,
+                                              y + ((code >> 10) & 3) - 1, z + ((code >> 12) & 3) - 1, d, &ok);
+                    val = ok ? w : fout;
+                    if (fl == 10 && m->link_value) {
+                        double* st = m->link_value + li * 2;
+                        const double cc = sqrt(1.0 / 3.0), fin = cc * st[0] + (1.0 - cc) * st[1];
+                        st[0] = val;
+                        st[1] = fin;
+                        val = fin;
+                    }
+                } else if (fl == 11 && m->link_value) {
+                    const double qd = m->link_value[li * 2];
+                    if (qd >= 0.5) {
+                        const double finv =
+                            f[gidx(gr, x + ooff[iq][0], y + ooff[iq][1], z + ooff[iq][2]) + oslot[iq] * gr->s[3]];
+                        val = 0.5 * (fout + finv * (2.0 * qd - 1.0)) / qd;
+                    } else if (qd > 0.0) {
+                        const double d2 = f_out_at(m, gr, periodic, ooff, oslot, f, x - m->c[q][0], y - m->c[q][1],
+                                                   z - m->c[q][2], q, &ok);
+                        val = 2.0 * qd * fout + (1.0 - 2.0 * qd) * (ok ? d2 : fout);
+                    }
+                }
             } else if (fl == 6 || fl == 7) {
                 double j[3] = {0.0, 0.0, 0.0}, u[3], feq[QMAX]; int k, d;
                 const double rw = fl == 6 ? fd_rho : m->fd_rho1;
@@ -747,7 +796,7 @@ int om_run(const om_method* m, const om_grid* gr, int pattern, int* parity, int 
     double *src = a, *dst = b;
     for (t = 0; t < steps; ++t) {
         om_periodic_sync(m, gr, pattern, *parity, periodic, src);
-        if (flags) om_boundaries(m, gr, pattern, *parity, flags, ubb_u, fd_rho, src);
+        if (flags) om_boundaries(m, gr, pattern, *parity, flags, ubb_u, fd_rho, periodic, src);
         *parity = inplace ? 1 - *parity : *parity;
         om_sweep(m, gr, pattern, *parity, src, inplace ? src : dst, flags, 0);
         if (!inplace) { double* tmp = src; src = dst; dst = tmp; swapped ^= 1; }

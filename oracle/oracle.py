@@ -52,6 +52,8 @@ class OmMethod(ctypes.Structure):
         ("ubb_density", ctypes.c_double),
         ("ubb_link", ctypes.c_void_p),
         ("fd_rho1", ctypes.c_double),
+        ("link_code", ctypes.c_void_p),
+        ("link_value", ctypes.c_void_p),
     ]
 
 
@@ -225,11 +227,13 @@ class Oracle:
 
     def run(self, f, steps, pattern="pull", parity=0, periodic=(True, True, True), flags=None,
             ubb_velocity=(0.0, 0.0, 0.0), tmp=None, fixed_density=1.0, ubb_link=None, ubb_adapt=False,
-            ubb_density=None, fixed_density1=1.0):
+            ubb_density=None, fixed_density1=1.0, link_code=None, link_value=None):
         """Runs `steps` time steps.  Returns (field holding the result, new parity).  Flags: 1 NoSlip,
         2 UBB (ubb_velocity, or per link ubb_link[x, y, z, q, 3] for the link from interior cell
         (x, y, z) in direction q; ubb_adapt shifts the wall velocity by -F/(2 rho_ref); ubb_density
-        prescribes the wall density), 6 / 7 FixedDensity (fixed_density / fixed_density1)."""
+        prescribes the wall density), 6 / 7 FixedDensity (fixed_density / fixed_density1), 8-11 FreeSlip,
+        SimpleExtrapolationOutflow, ExtrapolationOutflow, NoSlipLinearBouzidi with the per-link
+        link_code [x, y, z, Q] and link_value [x, y, z, Q, 2] (the outflow state is updated in a copy)."""
         g = self._grid(f)
         link = None
         if ubb_link is not None:
@@ -238,6 +242,13 @@ class Oracle:
         self._m.ubb_adapt = int(bool(ubb_adapt))
         self._m.ubb_density = float(ubb_density) if ubb_density else 0.0
         self._m.fd_rho1 = float(fixed_density1)
+        code = val = None
+        if link_code is not None:
+            code = np.ascontiguousarray(np.asarray(link_code, np.int32).transpose(2, 1, 0, 3))
+        if link_value is not None:
+            val = np.ascontiguousarray(np.asarray(link_value, np.float64).transpose(2, 1, 0, 3, 4))
+        self._m.link_code = code.ctypes.data if code is not None else None
+        self._m.link_value = val.ctypes.data if val is not None else None
         per = (ctypes.c_int * 3)(*[int(p) for p in periodic])
         par = ctypes.c_int(parity)
         ub = np.array(list(ubb_velocity) + [0.0] * (3 - len(ubb_velocity)), np.float64)
@@ -253,12 +264,12 @@ class Oracle:
                               steps, per, fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None
                               else None, self._ptr(ub), ctypes.c_double(fixed_density), self._ptr(f),
                               self._ptr(tmp))
-            self._m.ubb_link = None
+            self._m.ubb_link = self._m.link_code = self._m.link_value = None
             return (tmp if sw else f), par.value
         lib().om_run(ctypes.byref(self._m), ctypes.byref(g), PATTERNS[pattern], ctypes.byref(par), steps, per,
                      fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None else None,
                      self._ptr(ub), ctypes.c_double(fixed_density), self._ptr(f), self._ptr(f))
-        self._m.ubb_link = None
+        self._m.ubb_link = self._m.link_code = self._m.link_value = None
         return f, par.value
 
     def periodic_sync(self, f, pattern="pull", prev_parity=0, periodic=(True, True, True)):
