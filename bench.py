@@ -133,7 +133,7 @@ WORKLOADS = {
     "d3q27-cumulant-aa-channel-256x128x128": (lambda dev: make_channel(dev), SHAPE[0] * SHAPE[1] * SHAPE[2], 27, 4),
 }
 for _n in (64, 256, 512):
-    for _st, _isz in (("float64", 8), ("float32", 4), ("float16", 2), ("bfloat16", 2)):
+    for _st, _isz in (("float64", 8), ("float32", 4), ("float16", 2), ("bfloat16", 2), ("e3m12", 2)):
         WORKLOADS[f"d3q19-trt-pull-{_st}-{_n}"] = (
             (lambda dev, n=_n, st=_st: make_d3q19_tgv(dev, n, st)), _n ** 3, 19, _isz)
     WORKLOADS[f"d3q19-mrt-pull-float32-{_n}"] = (
@@ -155,6 +155,57 @@ def make_cavity_batch(device, n_cavities=512, seed=0):
 
 WORKLOADS["batched-ldc-512-d3q19-mrt-float32"] = (lambda dev: make_cavity_batch(dev), None, 19, 4)
 WORKLOADS["batched-ldc-64-d3q19-mrt-float32"] = (lambda dev: make_cavity_batch(dev, 64), None, 19, 4)
+
+
+class SparsePorousMedium:
+    """A periodic n^3 box filled with seeded random spheres (radius 3-7 cells, about a third of the
+    cells solid; the ghost layers mirror the solid cells of their periodic images), stored as a fluid-cell list with lbmpy's sparse layout (SparseLbMapper: NoSlip in
+    the index array), D3Q19 TRT FP32, force driven; one stream-pull-collide sweep of the list per
+    step (lbmpy_b200.sparse).  number_of_cells counts fluid cells."""
+
+    def __init__(self, device, n=192, seed=0):
+        import torch
+        import lbmpy_b200 as L
+        from lbmpy_b200 import sparse as S
+        rng = np.random.default_rng(seed)
+        ext = n + 2
+        solid = np.zeros((ext, ext, ext), bool)
+        ax = np.arange(ext)
+        centres = rng.uniform(1, n + 1, (int(0.02 * n ** 3 / 27), 3))
+        radii = rng.uniform(3, 7, len(centres))
+        for c, r in zip(centres, radii):
+            lo = np.maximum(np.floor(c - r).astype(int), 1)
+            hi = np.minimum(np.ceil(c + r).astype(int) + 1, n + 1)
+            X, Y, Z = np.meshgrid(ax[lo[0]:hi[0]], ax[lo[1]:hi[1]], ax[lo[2]:hi[2]], indexing="ij")
+            solid[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] |= (X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 < r * r
+        for a in range(3):      # ghost layers mirror their periodic images (a solid image bounces back)
+            sl = [slice(None)] * 3
+            src, dst = list(sl), list(sl)
+            src[a], dst[a] = n, 0
+            solid[tuple(dst)] = solid[tuple(src)]
+            src[a], dst[a] = 1, n + 1
+            solid[tuple(dst)] = solid[tuple(src)]
+        flags = np.zeros((ext, ext, ext), np.uint8)
+        flags[1:-1, 1:-1, 1:-1] = 1
+        flags[solid] = 2
+        kw = dict(relaxation_rate=1.8, compressible=False, force=(1e-6, 0, 0))
+        rule = L.create_lb_collision_rule(lbm_config=L.LBMConfig(stencil=L.Stencil.D3Q19, method=L.Method.TRT, **kw))
+        self.mapper = S.SparseLbMapper([tuple(d) for d in rule.method.stencil], flags, 1, 2, 0)
+        idx = self.mapper.create_index_array(1)
+        self.number_of_cells = self.mapper.num_fluid_cells
+        self.solid_fraction = float(solid[1:-1, 1:-1, 1:-1].mean())
+        self.kernel = S.create_lb_function_sparse(S.create_lb_update_rule_sparse(rule, "f", "d", "idx"))
+        self.f = S.pdf_list(len(self.mapper), 19, torch.float32, device)
+        self.d = S.pdf_list(len(self.mapper), 19, torch.float32, device)
+        S.create_macroscopic_value_setter_sparse(rule.method, "f", 1.0, (0.0, 0.0, 0.0))(self.f)
+        self.idx_host = idx
+
+    def time_step(self):
+        self.kernel(f=self.f, d=self.d, idx=self.idx_host)
+        self.f, self.d = self.d, self.f
+
+
+WORKLOADS["sparse-porous-192-d3q19-trt-float32"] = (lambda dev: SparsePorousMedium(dev), None, 19, 4)
 
 
 def make_closure_box(device, shape=(256, 128, 128)):
@@ -400,7 +451,8 @@ def main():
         del step
         torch.cuda.empty_cache()
         secondary = {}
-        for name in ("d3q19-trt-pull-float32-512", "d3q19-trt-pull-float16-512", "d3q19-trt-pull-bfloat16-512"):
+        for name in ("d3q19-trt-pull-float32-512", "d3q19-trt-pull-float16-512", "d3q19-trt-pull-bfloat16-512",
+                     "d3q19-trt-pull-e3m12-512"):
             f2, c2, q2, i2 = WORKLOADS[name]
             st2 = f2(device)
             for _ in range(4):
@@ -418,13 +470,37 @@ def main():
             torch.cuda.empty_cache()
         secondary["fp16_over_fp32"] = (secondary["d3q19-trt-pull-float16-512"]["GLUPS"] /
                                        secondary["d3q19-trt-pull-float32-512"]["GLUPS"])
+        secondary["e3m12_over_fp32"] = (secondary["d3q19-trt-pull-e3m12-512"]["GLUPS"] /
+                                        secondary["d3q19-trt-pull-float32-512"]["GLUPS"])
+        # other sweeps of the same family: weighted-orthogonal MRT (even/odd-paired transforms),
+        # and the sparse list sweep on a porous medium (bytes per fluid cell: Q reads, Q writes,
+        # Q - 1 four-byte indices)
+        for name, bpc in (("d3q19-mrt-pull-float32-256", 2 * 19 * 4), ("sparse-porous-192-d3q19-trt-float32",
+                                                                        2 * 19 * 4 + 18 * 4)):
+            st2 = WORKLOADS[name][0](device)
+            for _ in range(4):
+                st2.time_step()
+            a2, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a2.record(stream)
+            for _ in range(20):
+                st2.time_step()
+            b2.record(stream)
+            torch.cuda.synchronize()
+            g2 = st2.number_of_cells / (a2.elapsed_time(b2) / 20 * 1e-3) / 1e9
+            secondary[name] = {"GLUPS": g2, "GB/s": g2 * bpc, "frac": g2 * bpc / peak, "bytes_per_cell": bpc}
+            if name.startswith("sparse"):
+                secondary[name].update({"fluid_cells": st2.number_of_cells, "solid_fraction": st2.solid_fraction})
+            del st2
+            torch.cuda.empty_cache()
         if args.accuracy_steps > 0:
             # the same box from the same seeded state, stored in each type and in FP64 for the
             # reference: relative L2 velocity error after accuracy_steps sweeps (config c3: 5000)
             from lbmpy_b200.precision import precision_study
             acc = precision_study(512, args.accuracy_steps, args.accuracy_steps,
-                                  storages=("float32", "float16", "bfloat16"), device=device, log=lambda *_: None)
-            for st in ("float32", "float16", "bfloat16"):
+                                  storages=("float32", "float16", "bfloat16", "e3m12"), device=device,
+                                  log=lambda *_: None)
+            for st in ("float32", "float16", "bfloat16", "e3m12"):
                 secondary[f"d3q19-trt-pull-{st}-512"]["l2_vs_fp64"] = acc[st]["final_l2_velocity_error"]
                 secondary[f"d3q19-trt-pull-{st}-512"]["max_ke_rel_error"] = acc[st]["max_ke_rel_error"]
             secondary["accuracy_steps"] = args.accuracy_steps

@@ -39,8 +39,14 @@ enum {
 };
 
 enum { LBM_STENCIL_D3Q19 = 19, LBM_STENCIL_D3Q27 = 27 };
-enum { LBM_METHOD_SRT = 0, LBM_METHOD_TRT = 1, LBM_METHOD_MRT = 2, LBM_METHOD_CUMULANT = 3 };
-enum { LBM_DTYPE_F64 = 0, LBM_DTYPE_F32 = 1, LBM_DTYPE_F16 = 2, LBM_DTYPE_BF16 = 3 };
+/* CENTRAL_MOMENT: D3Q27 polynomial central moments relaxed about the equilibrium velocity
+ * (methods/momentbased/centralmomentbasedmethod.py:296-394), compressible, force models Guo / Luo /
+ * Simple applied in central-moment space; rates in the cumulant method's canonical order. */
+enum { LBM_METHOD_SRT = 0, LBM_METHOD_TRT = 1, LBM_METHOD_MRT = 2, LBM_METHOD_CUMULANT = 3,
+       LBM_METHOD_CENTRAL_MOMENT = 4 };
+/* E3M12: 16-bit float for zero-centred PDFs (sign, 3 exponent, 12 mantissa bits, scaled by 16;
+ * |value| < 1/16, relative step 2^-12, saturating); no lbmpy counterpart (lbmpy stores FP64 / FP32). */
+enum { LBM_DTYPE_F64 = 0, LBM_DTYPE_F32 = 1, LBM_DTYPE_F16 = 2, LBM_DTYPE_BF16 = 3, LBM_DTYPE_E3M12 = 4 };
 /* pull / push: two fields; AA, EsoTwist, EsoPull, EsoPush: in place (fieldaccess.py:66-318).
  * Push, EsoPull and EsoPush are built for FP64 / FP32 storage. */
 enum { LBM_PATTERN_PULL = 0, LBM_PATTERN_AA = 1, LBM_PATTERN_ESOTWIST = 2, LBM_PATTERN_PUSH = 3,
@@ -80,6 +86,12 @@ typedef struct LbmPlanDesc {
                                    boundaries/boundaryconditions.py:824-830) */
     uint32_t ubb_adapt_mask;    /* bit u: UBB number u shifts its wall velocity by -F/(2 rho_ref)
                                    (UBB(adapt_velocity_to_force=True), :790-794) */
+    double fourth_order_limiter; /* CUMULANT: > 0 applies the fourth-order correction (Geier et al.
+                                   2017; LBMConfig(fourth_order_correction=...),
+                                   methods/cumulantbased/fourth_order_correction.py:21-237) with this
+                                   limiter (lbmpy: 1e6 for True).  The rates of the third-order groups
+                                   (canonical 10-16) are then derived from the shear rate (rates[4])
+                                   and the bulk rate (rates[9]), those of orders 4-6 are 1. */
 } LbmPlanDesc;
 
 typedef struct LbmPlan LbmPlan;
@@ -266,6 +278,63 @@ int lbm_batch_sweep(const LbmBatch* batch, int parity, void* stream);
  * cells)}. */
 int lbm_batch_info(const LbmBatch* batch, int64_t info[4]);
 int lbm_batch_destroy(LbmBatch* batch);
+
+/* ---------------------------------------------------------------- sparse (list-based) domains
+ * Replaces lbmpy's sparse kernels (sparse/update_rule_sparse.py:22-52 create_lb_update_rule_sparse,
+ * :55-67 create_macroscopic_value_getter_sparse, :70-85 create_macroscopic_value_setter_sparse).
+ * The cells are a list of n_cells (n_fluid fluid cells first, then boundary cells); PDF i of list
+ * cell c is element c + i * n_cells of a PDF list.  `index` holds, for direction i = 1..Q-1 and
+ * fluid cell c, at index[(i - 1) * n_fluid + c], the element that cell c pulls population i from
+ * (lbmpy's SparseLbMapper.create_index_array (sparse/mapping.py:100-156), transposed from
+ * [n_fluid][Q-1] to [Q-1][n_fluid]); n_cells * Q must fit 32 bits.  The plan gives the stencil,
+ * method, rates, force, dtype (FP64 / FP32) and must use the pull pattern; its dims and flags
+ * play no part.  Boundary cells are neither read nor written by the sweep. */
+int lbm_sparse_sweep(const LbmPlan* plan, const void* src, void* dst, const uint32_t* index, int64_t n_fluid,
+                     int64_t n_cells, void* stream);
+/* Equilibrium of the fluid cells from rho[c] and u[k * n_fluid + c] (FP64 device arrays); the
+ * velocity enters unshifted by the force, as lbmpy's sparse setter builds it. */
+int lbm_sparse_set_equilibrium(const LbmPlan* plan, void* pdfs, const double* rho, const double* u,
+                               int64_t n_fluid, int64_t n_cells, void* stream);
+/* Velocity bounce-back on a PDF list before a sparse sweep (replaces the kernel lbmpy builds from
+ * SparseLbBoundaryMapper(UBB(...)), sparse/mapping.py:157-247): link k is the fluid cell
+ * links[n_links + k] with the direction links[k] (1..Q-1) pointing into the boundary cell
+ * links[2 * n_links + k]; slot inv(d) of the boundary cell receives
+ * f(c, d) - 6 w_d rho (c_d . velocity), rho the cell's density for compressible plans, else 1.
+ * Directions outside 1..Q-1 are skipped. */
+int lbm_sparse_ubb(const LbmPlan* plan, void* pdfs, const uint32_t* links, int64_t n_links, int64_t n_cells,
+                   const double velocity[3], void* stream);
+/* Density and velocity of the fluid cells into rho[c] and u[k * n_fluid + c] (FP64; either may
+ * be NULL). */
+int lbm_sparse_get_macroscopic(const LbmPlan* plan, const void* pdfs, double* rho, double* u, int64_t n_fluid,
+                               int64_t n_cells, void* stream);
+
+/* Staged sweep (LBM_VARIANT_STAGED): bound of each wait on a stage barrier, in ns (0: the default
+ * of 1 s).  A wait that runs out makes the sweep set LBM_STATUS_STAGE_TIMEOUT in the plan's
+ * status word (lbm_plan_status), leave the remaining cells of that CTA unswept and return.
+ * probe != 0 makes every CTA also wait, before its last tile, on a barrier that nothing arrives
+ * at, so that the bounded wait and the status report can be tested; 0 restores normal sweeps.
+ * No lbmpy counterpart. */
+int lbm_plan_set_stage_wait(LbmPlan* plan, uint64_t wait_ns, int probe);
+
+/* ---------------------------------------------------------------- slab decomposition
+ * Ghost-plane exchange of a z-slab (waLBerla-style block communication that lbmpy describes with
+ * get_communication_slices, advanced_streaming/communication.py:122-183, for the z faces).  A job
+ * copies slots slots[0..n_slots) of z-plane z (ghost-inclusive index, whole plane of
+ * nx_ext x ny_ext cells including the x/y ghost layers) between the PDF field and `buffer`, where
+ * element (k, y, x) sits at (k * ny_ext + y) * nx_ext + x: unpack == 0 packs the field into the
+ * buffer, unpack != 0 the reverse.  One launch runs every job; jobs must not write the same
+ * elements.  The field has Q = q slots of elem_size bytes (2, 4 or 8), nz_ext planes and the
+ * fzyx element strides {1, sy, sz, sq}. */
+#define LBM_HALO_MAX_JOBS 4
+typedef struct LbmHaloJob {
+    int32_t z;
+    int32_t unpack;
+    int32_t n_slots;
+    int32_t slots[27];
+    void* buffer;
+} LbmHaloJob;
+int lbm_halo_copy(void* pdfs, const int64_t strides[4], int32_t q, int32_t nx_ext, int32_t ny_ext, int32_t nz_ext,
+                  int32_t elem_size, const LbmHaloJob* jobs, int32_t n_jobs, void* stream);
 
 /* Copies the message of the last failed call on this thread into buf (NUL-terminated). */
 int lbm_last_error(char* buf, size_t n);

@@ -12,8 +12,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liblbmb200.so")
 
 LBM_OK, LBM_E_INVALID, LBM_E_CUDA, LBM_E_UNSUPPORTED, LBM_E_DEVICE = 0, 1, 2, 3, 4
-METHOD_SRT, METHOD_TRT, METHOD_MRT, METHOD_CUMULANT = 0, 1, 2, 3
-DTYPE_F64, DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2, 3
+METHOD_SRT, METHOD_TRT, METHOD_MRT, METHOD_CUMULANT, METHOD_CENTRAL_MOMENT = 0, 1, 2, 3, 4
+DTYPE_F64, DTYPE_F32, DTYPE_F16, DTYPE_BF16, DTYPE_E3M12 = 0, 1, 2, 3, 4
 PATTERN_PULL, PATTERN_AA, PATTERN_ESOTWIST, PATTERN_PUSH, PATTERN_ESOPULL, PATTERN_ESOPUSH = 0, 1, 2, 3, 4, 5
 FORCE_NONE, FORCE_GUO, FORCE_CENTRAL_MOMENT, FORCE_SIMPLE, FORCE_LUO = 0, 1, 2, 3, 4
 SGS_NONE, SGS_SMAGORINSKY, SGS_MLP = 0, 1, 2
@@ -28,6 +28,8 @@ EXPORTS = ("lbm_plan_create", "lbm_plan_destroy", "lbm_plan_update", "lbm_plan_s
            "lbm_set_equilibrium", "lbm_get_macroscopic", "lbm_reduce_conserved", "lbm_reduce_conserved_noalloc",
            "lbm_flags_finalize", "lbm_plan_set_links", "lbm_closure_set_weights", "lbm_closure_features", "lbm_mlp_forward",
            "lbm_mlp_create", "lbm_mlp_destroy", "lbm_mlp_loss_grad", "lbm_mlp_adam", "lbm_batch_create", "lbm_batch_sweep", "lbm_batch_info", "lbm_batch_destroy",
+           "lbm_sparse_sweep", "lbm_sparse_set_equilibrium", "lbm_sparse_get_macroscopic", "lbm_sparse_ubb",
+           "lbm_plan_set_stage_wait", "lbm_halo_copy",
            "lbm_last_error", "lbm_version")
 
 
@@ -51,6 +53,7 @@ class LbmPlanDesc(ctypes.Structure):
         ("fixed_density1", ctypes.c_double),
         ("ubb_density", ctypes.c_double * 4),
         ("ubb_adapt_mask", ctypes.c_uint32),
+        ("fourth_order_limiter", ctypes.c_double),
     ]
 
 
@@ -65,6 +68,14 @@ class LbmDomainDesc(ctypes.Structure):
         ("strides", ctypes.c_int64 * 4), ("offset", ctypes.c_int64), ("flags_offset", ctypes.c_int64),
         ("rates", ctypes.c_double * 27), ("ubb_velocity", (ctypes.c_double * 3) * 4),
     ]
+
+
+HALO_MAX_JOBS = 4
+
+
+class LbmHaloJob(ctypes.Structure):
+    _fields_ = [("z", ctypes.c_int32), ("unpack", ctypes.c_int32), ("n_slots", ctypes.c_int32),
+                ("slots", ctypes.c_int32 * 27), ("buffer", ctypes.c_void_p)]
 
 
 class LbmBatchTiling(ctypes.Structure):
@@ -116,6 +127,13 @@ def lib():
         L.lbm_batch_sweep.argtypes = [vp, ctypes.c_int, vp]
         L.lbm_batch_info.argtypes = [vp, i64p]
         L.lbm_batch_destroy.argtypes = [vp]
+        L.lbm_sparse_sweep.argtypes = [vp, vp, vp, vp, ctypes.c_int64, ctypes.c_int64, vp]
+        L.lbm_sparse_set_equilibrium.argtypes = [vp, vp, vp, vp, ctypes.c_int64, ctypes.c_int64, vp]
+        L.lbm_sparse_get_macroscopic.argtypes = [vp, vp, vp, vp, ctypes.c_int64, ctypes.c_int64, vp]
+        L.lbm_sparse_ubb.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(ctypes.c_double), vp]
+        L.lbm_plan_set_stage_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_int]
+        L.lbm_halo_copy.argtypes = [vp, i64p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                    ctypes.c_int32, ctypes.POINTER(LbmHaloJob), ctypes.c_int32, vp]
         L.lbm_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTS:
             getattr(L, name).restype = ctypes.c_int

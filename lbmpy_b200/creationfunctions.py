@@ -185,7 +185,9 @@ class LBMOptimisation:
     builtin_periodicity: Tuple[bool, ...] = (False, False, False)
     storage_dtype: Any = None
     """PDF storage type when it differs from the arithmetic type (``CreateKernelConfig.data_type``):
-    'float16' / 'bfloat16' store zero-centred PDFs in 16 bits and collide in FP32."""
+    'float16' / 'bfloat16' / 'e3m12' store zero-centred PDFs in 16 bits and collide in FP32.  e3m12
+    (sign, 3 exponent, 12 mantissa bits, scaled by 16) keeps four times finer steps than float16 for
+    |f - w| < 1/16 and saturates beyond."""
 
 
 @dataclass
@@ -294,12 +296,12 @@ def create_lb_method(lbm_config=None, **params):
         raise NotImplementedError(f"the B200 sweep is built for D3Q19 and D3Q27, not {st.name}")
     if lbm_config.entropic or lbm_config.fluctuating or lbm_config.cassons or lbm_config.psm_config:
         raise NotImplementedError("entropic, fluctuating, Casson and PSM collision add-ons are not built")
-    if lbm_config.fourth_order_correction:
-        raise NotImplementedError("the fourth-order cumulant correction is not built")
     if lbm_config.nested_moments is not None:
         raise NotImplementedError("custom moment sets are not built; the default bases are")
     if not lbm_config.zero_centered:
         raise NotImplementedError("the B200 sweep stores zero-centred PDFs (zero_centered=True)")
+    if lbm_config.fourth_order_correction and (lbm_config.method != Method.CUMULANT or st.name != "D3Q27"):
+        raise ValueError("Fourth-order correction can only be applied to D3Q27 cumulant methods.")
     rates = list(lbm_config.relaxation_rates)
     method = lbm_config.method
     dim = st.D
@@ -330,11 +332,34 @@ def create_lb_method(lbm_config=None, **params):
     elif method == Method.CUMULANT:
         if st.name != "D3Q27":
             raise NotImplementedError("the cumulant sweep is built for D3Q27")
+        if lbm_config.fourth_order_correction:
+            # creationfunctions.py:696-707, :835-846: shear and bulk rate (bulk 1 by default), the
+            # optimal third-order rates, 1 for orders 4-6 (the sweep limits the third-order rates
+            # per cell and adds the fourth-order correction terms)
+            assert len(rates) <= 2, ("Optimal parametrisation for fourth-order cumulants needs either one or two "
+                                     "relaxation rates, associated with the shear (and bulk) viscosity. All other "
+                                     "relaxation rates are automatically chosen optimally")
+            w1 = rates[0]
+            w2 = rates[1] if len(rates) > 1 else 1
+            (w3, w4, w5), _ = M.fourth_order_rates(w1, w2)
+            rates = [w1, w2, w3, w4, w5, 1, 1, 1, 1, 1]
         groups = M.cumulant_groups()
         per = M.rates_for_groups(rates, groups, dim, lbm_config.conserved_moments) if all(
             _is_number(r) for r in rates) else _symbolic_rates_for_groups(rates, groups, dim,
                                                                            lbm_config.conserved_moments)
         kind = "cumulant"
+    elif method == Method.CENTRAL_MOMENT:
+        # creationfunctions.py:818-822, methods/creationfunctions.py:336-381: the default D3Q27 central
+        # moment groups (default_moment_sets.py:110-148) are the cumulant groups
+        if st.name != "D3Q27":
+            raise NotImplementedError("the central-moment sweep is built for D3Q27")
+        if not lbm_config.compressible:
+            raise NotImplementedError("the central-moment sweep is built for compressible methods")
+        groups = M.cumulant_groups()
+        per = M.rates_for_groups(rates, groups, dim, lbm_config.conserved_moments) if all(
+            _is_number(r) for r in rates) else _symbolic_rates_for_groups(rates, groups, dim,
+                                                                           lbm_config.conserved_moments)
+        kind = "central_moment"
     else:
         raise NotImplementedError(f"method {method} is not built for the B200 sweep")
     fm = lbm_config.force_model
@@ -372,6 +397,7 @@ class LbmCollisionRule:
     output: dict = field(default_factory=dict)
     closure: Any = None               # MLPClosure for SubgridScaleModel.LEARNED
     simplification_hints: dict = field(default_factory=dict)
+    fourth_order_limiter: float = 0.0  # > 0: fourth-order cumulant correction with this limiter
 
 
 def create_lb_collision_rule(lb_method=None, lbm_config=None, lbm_optimisation=None, config=None,
@@ -402,20 +428,28 @@ def create_lb_collision_rule(lb_method=None, lbm_config=None, lbm_optimisation=N
                 raise NotImplementedError("the learned closure is built for the D3Q27 cumulant method")
         elif sgs != SubgridScaleModel.SMAGORINSKY:
             raise NotImplementedError("the Smagorinsky and learned subgrid-scale models are built")
+    foc = 0.0
+    if lbm_config.fourth_order_correction:
+        # creationfunctions.py:696-707: True means limiters of 1e6 (practically none)
+        if lb_method.kind != "cumulant" or lb_method.stencil.name != "D3Q27":
+            raise ValueError("Fourth-order correction is only defined for D3Q27 cumulant methods.")
+        if sgs is not None:
+            raise NotImplementedError("the fourth-order correction is not built with subgrid-scale models")
+        foc = 1e6 if lbm_config.fourth_order_correction is True else float(lbm_config.fourth_order_correction)
     rule = LbmCollisionRule(lb_method, bool(lbm_config.galilean_correction), sgs, c, dict(lbm_config.output),
-                            closure=closure)
+                            closure=closure, fourth_order_limiter=foc)
     lbm_config.collision_rule = rule
     return rule
 
 
 # ---------------------------------------------------------------------------- update rule
 _DTYPES = {"float64": N.DTYPE_F64, "double": N.DTYPE_F64, "float32": N.DTYPE_F32, "float": N.DTYPE_F32,
-           "float16": N.DTYPE_F16, "half": N.DTYPE_F16, "bfloat16": N.DTYPE_BF16}
+           "float16": N.DTYPE_F16, "half": N.DTYPE_F16, "bfloat16": N.DTYPE_BF16, "e3m12": N.DTYPE_E3M12}
 
 
 def _dtype_name(dt) -> str:
     s = str(dt)
-    for k in ("bfloat16", "float16", "float32", "float64"):
+    for k in ("bfloat16", "float16", "float32", "float64", "e3m12"):
         if k in s:
             return k
     if s in ("double",):
@@ -471,11 +505,11 @@ def create_lb_update_rule(collision_rule=None, lbm_config=None, lbm_optimisation
     storage = _dtype_name(lbm_optimisation.storage_dtype) if lbm_optimisation.storage_dtype else data_type
     if data_type not in ("float64", "float32"):
         raise ValueError("the arithmetic type (CreateKernelConfig.data_type) must be float64 or float32")
-    if storage in ("float16", "bfloat16") and data_type != "float32":
+    if storage in ("float16", "bfloat16", "e3m12") and data_type != "float32":
         raise ValueError("16-bit PDF storage collides in float32: set data_type='float32'")
     if storage == "float64" and data_type != "float64" or storage == "float32" and data_type != "float32":
         raise ValueError("storage_dtype must match data_type unless it is a 16-bit type")
-    if storage in ("float16", "bfloat16") and pattern in ("push", "esopull", "esopush"):
+    if storage in ("float16", "bfloat16", "e3m12") and pattern in ("push", "esopull", "esopush"):
         raise NotImplementedError(f"streaming pattern {pattern!r} is built for float64 / float32 storage")
     rule = LbmUpdateRule(collision_rule, pattern, lbm_config.timestep, lbm_config.field_name,
                          lbm_config.temporary_field_name, data_type, storage,

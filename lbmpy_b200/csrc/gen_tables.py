@@ -49,15 +49,27 @@ def generate() -> str:
         for d, axis in enumerate("xyz"):
             out.append(_array_fn(pre + "c" + axis, [str(v[d]) for v in dirs], "int"))
         out.append(_array_fn(pre + "inv", [str(v) for v in inv], "int"))
+        # one representative direction per pair of opposite directions (the lower index)
+        out.append(_array_fn(pre + "pair", [str(i) for i in range(1, q) if i < inv[i]], "int"))
         out.append(_array_fn(pre + "w", [_f(v) for v in w]))
         for cont, tag in ((True, "cont"), (False, "disc")):
             _, lin, quad = M.population_equilibrium(name, cont)
             out.append(_array_fn(pre + "eqlin_" + tag, [_f(v) for r in lin for v in r], nidx=2, dims=(q, 3)))
             out.append(_array_fn(pre + "eqquad_" + tag, [_f(v) for r in quad for v in r], nidx=2, dims=(q, 6)))
         groups, Mm, Minv, eq = M.mrt_tables(name)
+        # the sweep transforms sums and differences of opposite populations: every row of M must be
+        # even or odd under c -> -c, and column k of M^-1 must share row k's parity
+        for k in range(q):
+            ev = all(Mm[k][i] == Mm[k][inv[i]] for i in range(q))
+            od = all(Mm[k][i] == -Mm[k][inv[i]] for i in range(q))
+            assert ev != od, f"{name} MRT row {k} has no definite parity"
+            assert all(Minv[i][k] == (1 if ev else -1) * Minv[inv[i]][k] for i in range(q)), \
+                f"{name} MRT inverse column {k} breaks the parity of row {k}"
         gid = [gi for gi, g in enumerate(groups) for _ in g]
         out.append(f"constexpr int {pre}mrt_ngroups = {len(groups)};")
         out.append(_array_fn(pre + "mrt_group", [str(v) for v in gid], "int"))
+        even = [int(all(Mm[k][i] == Mm[k][inv[i]] for i in range(q))) for k in range(q)]
+        out.append(_array_fn(pre + "mrt_even", [str(v) for v in even], "int"))
         out.append(_array_fn(pre + "mrt_M", [_f(v) for r in Mm for v in r], nidx=2, dims=(q, q)))
         out.append(_array_fn(pre + "mrt_Minv", [_f(v) for r in Minv for v in r], nidx=2, dims=(q, q)))
         out.append(_array_fn(pre + "mrt_p0", [_f(e[0]) for e in eq]))

@@ -2,6 +2,7 @@
 // configuration and the macroscopic / reduction / flag kernels that do not depend on the method.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdarg>
 #include <cstdint>
 #include <cstdlib>
@@ -37,6 +38,8 @@ struct LbmPlan {
     const int* link_code;
     double* link_value;
     uint32_t ubb_link_mask;
+    unsigned long long stage_wait_ns;   // bound of the staged sweep's barrier waits (0: default)
+    int stage_probe;                    // staged sweep: wait on a barrier nothing arrives at (test)
     Physics phys;
     double* partial;       // reduction scratch: RED_BLOCKS * 5 doubles
     double* red_out;       // 5 doubles on the device
@@ -160,6 +163,7 @@ SweepLauncher sweep_launcher(const LbmPlan* p, int pat) {
     if (p->q == 27 && p->mk == MK_CUM) return sweep_q27_cum(p->store, pat);
     if (p->q == 27 && p->mk == MK_CUM1) return sweep_q27_cum1(p->store, pat);
     if (p->q == 27 && p->mk == MK_CUM1_MLP) return sweep_q27_closure(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CM) return sweep_q27_cm(p->store, pat);
     return nullptr;
 }
 
@@ -196,7 +200,7 @@ SweepLauncher quad_launcher(const LbmPlan* p, int pat) {
 bool quad_applicable(const LbmPlan* p, const void* src, const void* dst, const int64_t s[4], int pat,
                      const float* omega_out) {
     if (p->use_quad == 0 || (p->use_quad < 0 && p->mk != MK_POP)) return false;
-    if (p->store != ST_F16 && p->store != ST_BF16) return false;
+    if (p->store != ST_F16 && p->store != ST_BF16 && p->store != ST_E3M12) return false;
     if (omega_out != nullptr || (pat != PAT_PULL && pat != PAT_AA_EVEN && pat != PAT_AA_ODD)) return false;
     if (p->desc.dims[0] % 4 != 0) return false;
     const size_t es = store_size(p->store);
@@ -213,7 +217,7 @@ bool quad_applicable(const LbmPlan* p, const void* src, const void* dst, const i
 // one-cell sweep already streams at HBM speed and keeps twice the occupancy.
 bool pair_preferred(const LbmPlan* p, int pat) {
     if (p->use_pair >= 0) return p->use_pair == 1;
-    if (p->store == ST_F16 || p->store == ST_BF16) return true;
+    if (p->store == ST_F16 || p->store == ST_BF16 || p->store == ST_E3M12) return true;
     return (p->mk == MK_CUM || p->mk == MK_CUM1) && pat == PAT_PULL;
 }
 
@@ -229,13 +233,14 @@ bool pair_applicable(const LbmPlan* p, const void* src, const void* dst, const i
     return pair_launcher(p, pat) != nullptr;
 }
 
-SweepLauncher fixed_density_launcher(const LbmPlan* p, int pat) {
-    if (p->q == 19 && p->mk == MK_POP) return fixed_density_q19_pop(p->store, pat);
-    if (p->q == 19 && p->mk == MK_MRT) return fixed_density_q19_mrt(p->store, pat);
-    if (p->q == 27 && p->mk == MK_POP) return fixed_density_q27_pop(p->store, pat);
-    if (p->q == 27 && p->mk == MK_MRT) return fixed_density_q27_mrt(p->store, pat);
-    if (p->q == 27 && p->mk == MK_CUM) return fixed_density_q27_cum(p->store, pat);
-    if (p->q == 27 && (p->mk == MK_CUM1 || p->mk == MK_CUM1_MLP)) return fixed_density_q27_cum1(p->store, pat);
+SweepLauncher prepass_launcher(const LbmPlan* p, int pat) {
+    if (p->q == 19 && p->mk == MK_POP) return prepass_q19_pop(p->store, pat);
+    if (p->q == 19 && p->mk == MK_MRT) return prepass_q19_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_POP) return prepass_q27_pop(p->store, pat);
+    if (p->q == 27 && p->mk == MK_MRT) return prepass_q27_mrt(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CUM) return prepass_q27_cum(p->store, pat);
+    if (p->q == 27 && (p->mk == MK_CUM1 || p->mk == MK_CUM1_MLP)) return prepass_q27_cum1(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CM) return prepass_q27_cm(p->store, pat);
     return nullptr;
 }
 
@@ -274,6 +279,7 @@ MacroLauncher set_eq_launcher(const LbmPlan* p, int pat) {
     if (p->q == 27 && p->mk == MK_MRT) return set_eq_q27_mrt(p->store, pat);
     if (p->q == 27 && (p->mk == MK_CUM || p->mk == MK_CUM1 || p->mk == MK_CUM1_MLP))
         return set_eq_q27_cum(p->store, pat);
+    if (p->q == 27 && p->mk == MK_CM) return set_eq_q27_cm(p->store, pat);
     return nullptr;
 }
 
@@ -312,6 +318,7 @@ MacroLauncher get_launcher_q(int store, int pat) {
         case ST_F32: return pick_get<float, float, Q>(pat);
         case ST_F16: return pick_get<__half, float, Q>(pat);
         case ST_BF16: return pick_get<__nv_bfloat16, float, Q>(pat);
+        case ST_E3M12: return pick_get<e3m12, float, Q>(pat);
     }
     return nullptr;
 }
@@ -352,6 +359,7 @@ ReduceLauncher reduce_launcher_q(int store, int pat) {
         case ST_F32: return pick_reduce<float, Q>(pat);
         case ST_F16: return pick_reduce<__half, Q>(pat);
         case ST_BF16: return pick_reduce<__nv_bfloat16, Q>(pat);
+        case ST_E3M12: return pick_reduce<e3m12, Q>(pat);
     }
     return nullptr;
 }
@@ -393,6 +401,7 @@ UbbLauncher ubb_launcher_q(int store, int pat) {
         case ST_F32: return pick_ubb<float, float, Q>(pat);
         case ST_F16: return pick_ubb<__half, float, Q>(pat);
         case ST_BF16: return pick_ubb<__nv_bfloat16, float, Q>(pat);
+        case ST_E3M12: return pick_ubb<e3m12, float, Q>(pat);
     }
     return nullptr;
 }
@@ -463,6 +472,26 @@ __global__ void k_flags_finalize(Grid g) {
     fl[fc] = (uint8_t)v;
 }
 
+// Optimal third-order rates w3..w5 (before the per-cell limiters) and the parameters a, b of the
+// fourth-order correction for shear rate w1 and bulk rate w2 (Geier et al. 2017, eq. 111-116;
+// methods/cumulantbased/fourth_order_correction.py:79-97, :149-170).  False if a denominator vanishes.
+bool fourth_order_params(double w1, double w2, double w[3], double ab[2]) {
+    const double w11 = w1 * w1, w12 = w1 * w2, w22 = w2 * w2;
+    const double d3 = 8.0 * (5.0 - 2.0 * w1) * w1 + w2 * (8.0 + w1 * (9.0 * w1 - 26.0));
+    const double d4 = w2 * (56.0 - 42.0 * w1 + 9.0 * w11) - 8.0 * w1;
+    const double d5 = 16.0 * w11 * (w1 - 6.0) - 2.0 * w12 * (216.0 + 5.0 * w1 * (9.0 * w1 - 46.0)) +
+                      w22 * (w1 * (3.0 * w1 - 10.0) * (15.0 * w1 - 28.0) - 48.0);
+    const double dab = (w1 - w2) * (w2 * (2.0 + 3.0 * w1) - 8.0 * w1);
+    if (d3 == 0.0 || d4 == 0.0 || d5 == 0.0 || dab == 0.0) return false;
+    w[0] = 8.0 * (w1 - 2.0) * (w2 * (3.0 * w1 - 1.0) - 5.0 * w1) / d3;
+    w[1] = 8.0 * (w1 - 2.0) * (w1 + w2 * (3.0 * w1 - 7.0)) / d4;
+    w[2] = 24.0 * (w1 - 2.0) * (4.0 * w11 + w12 * (18.0 - 13.0 * w1) + w22 * (2.0 + w1 * (6.0 * w1 - 11.0))) / d5;
+    ab[0] = (4.0 * w11 + 2.0 * w12 * (w1 - 6.0) + w22 * (w1 * (10.0 - 3.0 * w1) - 4.0)) / dab;
+    ab[1] = (4.0 * w12 * (9.0 * w1 - 16.0) - 4.0 * w11 - 2.0 * w22 * (2.0 + 9.0 * w1 * (w1 - 2.0))) / (3.0 * dab);
+    return std::isfinite(w[0]) && std::isfinite(w[1]) && std::isfinite(w[2]) && std::isfinite(ab[0]) &&
+           std::isfinite(ab[1]);
+}
+
 int fill_physics(LbmPlan* p, const LbmPlanDesc* d) {
     Physics& ph = p->phys;
     memset(&ph, 0, sizeof(ph));
@@ -484,6 +513,17 @@ int fill_physics(LbmPlan* p, const LbmPlanDesc* d) {
     for (int u = 0; u < MAX_UBB; ++u) ph.ubb_density[u] = d->ubb_density[u];
     ph.ubb_adapt_mask = d->ubb_adapt_mask & 0xfu;
     ph.ubb_link_mask = p->ubb_link_mask;
+    if (d->method == LBM_METHOD_CUMULANT && d->fourth_order_limiter > 0.0) {
+        double w[3], ab[2];
+        fourth_order_params(d->rates[4], d->rates[9], w, ab);
+        for (int k = 10; k < 13; ++k) ph.rates[k] = w[0];
+        for (int k = 13; k < 16; ++k) ph.rates[k] = w[1];
+        ph.rates[16] = w[2];
+        for (int k = 17; k < 27; ++k) ph.rates[k] = 1.0;
+        ph.foc_limiter = d->fourth_order_limiter;
+        ph.foc_a = ab[0];
+        ph.foc_b = ab[1];
+    }
     return LBM_OK;
 }
 
@@ -499,19 +539,43 @@ bool cumulant_high_orders_relax_to_equilibrium(const LbmPlanDesc* d) {
 
 int method_kind(const LbmPlanDesc* d) {
     if (d->method == LBM_METHOD_MRT) return MK_MRT;
+    if (d->method == LBM_METHOD_CENTRAL_MOMENT) return MK_CM;
     if (d->method != LBM_METHOD_CUMULANT) return MK_POP;
-    if (!cumulant_high_orders_relax_to_equilibrium(d)) return MK_CUM;
+    if (d->fourth_order_limiter > 0.0 || !cumulant_high_orders_relax_to_equilibrium(d)) return MK_CUM;
     return d->sgs == LBM_SGS_MLP ? MK_CUM1_MLP : MK_CUM1;
 }
 
 int validate_desc(const LbmPlanDesc* d) {
     if (d->stencil != 19 && d->stencil != 27) return fail(LBM_E_UNSUPPORTED, "stencil must be D3Q19 or D3Q27");
-    if (d->method < 0 || d->method > 3) return fail(LBM_E_INVALID, "unknown method %d", d->method);
+    if (d->method < 0 || d->method > 4) return fail(LBM_E_INVALID, "unknown method %d", d->method);
+    if (d->method == LBM_METHOD_CENTRAL_MOMENT) {
+        if (d->stencil != 27) return fail(LBM_E_UNSUPPORTED, "the central-moment sweep is built for D3Q27 only");
+        if (!d->compressible)
+            return fail(LBM_E_UNSUPPORTED, "the central-moment sweep is built for compressible methods");
+        if (d->sgs != LBM_SGS_NONE)
+            return fail(LBM_E_UNSUPPORTED, "subgrid-scale models are not built for the central-moment sweep");
+        if (d->store_dtype != LBM_DTYPE_F64 && d->store_dtype != LBM_DTYPE_F32)
+            return fail(LBM_E_UNSUPPORTED, "the central-moment sweep is built for FP64 and FP32 storage");
+        if (d->pattern != LBM_PATTERN_PULL && d->pattern != LBM_PATTERN_AA)
+            return fail(LBM_E_UNSUPPORTED, "the central-moment sweep is built for the pull and AA patterns");
+    }
     if (d->method == LBM_METHOD_CUMULANT && d->stencil != 27)
         return fail(LBM_E_UNSUPPORTED, "the cumulant sweep is built for D3Q27 only");
+    if (!(d->fourth_order_limiter >= 0.0))
+        return fail(LBM_E_INVALID, "fourth_order_limiter must be >= 0 (0: no fourth-order correction)");
+    if (d->fourth_order_limiter > 0.0) {
+        if (d->method != LBM_METHOD_CUMULANT)
+            return fail(LBM_E_INVALID, "Fourth-order correction can only be applied to D3Q27 cumulant methods.");
+        if (d->sgs != LBM_SGS_NONE)
+            return fail(LBM_E_UNSUPPORTED, "the fourth-order correction is not built with subgrid-scale models");
+        double w[3], ab[2];
+        if (!fourth_order_params(d->rates[4], d->rates[9], w, ab))
+            return fail(LBM_E_INVALID, "the fourth-order correction is undefined for shear rate %g and bulk rate %g",
+                        d->rates[4], d->rates[9]);
+    }
     if (d->method == LBM_METHOD_CUMULANT && !d->compressible)
         return fail(LBM_E_INVALID, "Incompressible cumulant-based methods are not supported (yet).");
-    if (d->store_dtype < 0 || d->store_dtype > 3) return fail(LBM_E_INVALID, "unknown dtype %d", d->store_dtype);
+    if (d->store_dtype < 0 || d->store_dtype > 4) return fail(LBM_E_INVALID, "unknown dtype %d", d->store_dtype);
     if (d->pattern < 0 || d->pattern > 5) return fail(LBM_E_INVALID, "unknown streaming pattern %d", d->pattern);
     if (d->force_model < 0 || d->force_model > 4) return fail(LBM_E_INVALID, "unknown force model");
     if (d->method == LBM_METHOD_CUMULANT && d->force_model != LBM_FORCE_NONE &&
@@ -604,6 +668,8 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
     p->link_code = nullptr;
     p->link_value = nullptr;
     p->ubb_link_mask = 0;
+    p->stage_wait_ns = 0;
+    p->stage_probe = 0;
     fill_physics(p, desc);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
@@ -698,7 +764,8 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
     a.dst = dst;
     a.omega_out = omega_out;
     a.zc = (p->mk == MK_CUM1_MLP && p->store == ST_F32) ? p->zc : 1;
-    a.pad_ = 0;
+    a.stage_probe = p->stage_probe;
+    a.stage_wait_ns = p->stage_wait_ns;
     a.ubb_rho = nullptr;
     a.status = p->status;
     a.ubb_block = p->ubb_block;
@@ -715,13 +782,14 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
         if (e != cudaSuccess) return cuda_fail(e, "wall-density launch");
         a.ubb_rho = p->ubb_rho;
     }
-    if (flags != nullptr && (p->desc.fixed_density > 0 || p->desc.fixed_density1 > 0)) {
-        SweepLauncher F = fixed_density_launcher(p, pat);
-        if (F == nullptr) return fail(LBM_E_UNSUPPORTED, "no FixedDensity kernel for this storage type / pattern");
+    if (flags != nullptr && (p->desc.fixed_density > 0 || p->desc.fixed_density1 > 0 || p->link_code != nullptr ||
+                             p->link_value != nullptr)) {
+        SweepLauncher F = prepass_launcher(p, pat);
+        if (F == nullptr) return fail(LBM_E_UNSUPPORTED, "no boundary pre-pass kernel for this storage type / pattern");
         dim3 fg, fb;
         launch_shape(a.g, 1, fg, fb);
         cudaError_t e = F(a, fg, fb, stream);
-        if (e != cudaSuccess) return cuda_fail(e, "FixedDensity launch");
+        if (e != cudaSuccess) return cuda_fail(e, "boundary pre-pass launch");
     }
     const int variant = sweep_variant(p, src, dst, strides, pat, omega_out);
     if (variant == LBM_VARIANT_STAGED) {
@@ -918,6 +986,14 @@ int lbm_flags_finalize(const LbmPlan* p, uint8_t* flags, void* stream) {
     return LBM_OK;
 }
 
+int lbm_plan_set_stage_wait(LbmPlan* p, uint64_t wait_ns, int probe) {
+    if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
+    if (wait_ns > 60ull * 1000000000ull) return fail(LBM_E_INVALID, "wait_ns above 60 s");
+    p->stage_wait_ns = wait_ns;
+    p->stage_probe = probe ? 1 : 0;
+    return LBM_OK;
+}
+
 int lbm_plan_set_links(LbmPlan* p, const LbmLinkTables* t) {
     if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
     int rc;
@@ -948,6 +1024,145 @@ int lbm_plan_set_links(LbmPlan* p, const LbmLinkTables* t) {
 
 }  // extern "C"
 
+// ------------------------------------------------------------------ sparse (list-based) domains
+namespace {
+
+SparseLauncher sparse_launcher(const LbmPlan* p) {
+    if (p->q == 19 && p->mk == MK_POP) return sparse_q19_pop(p->store);
+    if (p->q == 19 && p->mk == MK_MRT) return sparse_q19_mrt(p->store);
+    if (p->q == 27 && p->mk == MK_POP) return sparse_q27_pop(p->store);
+    if (p->q == 27 && p->mk == MK_MRT) return sparse_q27_mrt(p->store);
+    if (p->q == 27 && p->mk == MK_CUM) return sparse_q27_cum(p->store);
+    if (p->q == 27 && p->mk == MK_CUM1) return sparse_q27_cum1(p->store);
+    if (p->q == 27 && p->mk == MK_CM) return sparse_q27_cm(p->store);
+    return nullptr;
+}
+
+SparseSetLauncher sparse_set_launcher(const LbmPlan* p) {
+    if (p->q == 19 && p->mk == MK_POP) return sparse_set_q19_pop(p->store);
+    if (p->q == 19 && p->mk == MK_MRT) return sparse_set_q19_mrt(p->store);
+    if (p->q == 27 && p->mk == MK_POP) return sparse_set_q27_pop(p->store);
+    if (p->q == 27 && p->mk == MK_MRT) return sparse_set_q27_mrt(p->store);
+    if (p->q == 27 && (p->mk == MK_CUM || p->mk == MK_CUM1)) return sparse_set_q27_cum(p->store);
+    if (p->q == 27 && p->mk == MK_CM) return sparse_set_q27_cm(p->store);
+    return nullptr;
+}
+
+template <class S, class R, int Q>
+cudaError_t launch_sparse_get(const SparseArgs& a, double* rho, double* u, cudaStream_t s) {
+    k_sparse_get_macroscopic<S, R, Q><<<(unsigned)((a.n_fluid + 255) / 256), 256, 0, s>>>(a, rho, u);
+    return cudaGetLastError();
+}
+
+template <class S, class R, int Q>
+cudaError_t launch_sparse_ubb(const SparseArgs& a, const uint32_t* links, int64_t n, const double* u,
+                              cudaStream_t s) {
+    k_sparse_ubb<S, R, Q><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, links, n, u[0], u[1], u[2]);
+    return cudaGetLastError();
+}
+
+int sparse_common(const LbmPlan* p, const void* src, const void* dst, int64_t n_fluid, int64_t n_cells,
+                  SparseArgs& a) {
+    if (p == nullptr) return fail(LBM_E_INVALID, "plan is NULL");
+    int rc;
+    if ((rc = check_device(p))) return rc;
+    if (p->store != ST_F64 && p->store != ST_F32)
+        return fail(LBM_E_UNSUPPORTED, "sparse domains are built for FP64 and FP32 storage");
+    if (p->desc.pattern != LBM_PATTERN_PULL)
+        return fail(LBM_E_UNSUPPORTED, "sparse domains stream by the pull pattern (the index list encodes it)");
+    if (p->desc.sgs == LBM_SGS_MLP)
+        return fail(LBM_E_UNSUPPORTED, "the learned closure is not built for sparse domains");
+    if (n_fluid < 0 || n_cells < n_fluid)
+        return fail(LBM_E_INVALID, "need 0 <= n_fluid <= n_cells (got %lld, %lld)", (long long)n_fluid,
+                    (long long)n_cells);
+    if (n_cells * (int64_t)p->q > (int64_t)UINT32_MAX)
+        return fail(LBM_E_INVALID, "n_cells * Q must fit the 32-bit index list");
+    if (n_fluid / 256 >= (int64_t)INT32_MAX) return fail(LBM_E_INVALID, "too many fluid cells for one launch");
+    if ((rc = check_device_ptr(p, src, "src", false))) return rc;
+    if ((rc = check_device_ptr(p, dst, "dst", false))) return rc;
+    memset(&a, 0, sizeof(a));
+    a.p = p->phys;
+    a.src = src;
+    a.dst = const_cast<void*>(dst);
+    a.n_fluid = n_fluid;
+    a.n_cells = n_cells;
+    return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_sparse_sweep(const LbmPlan* p, const void* src, void* dst, const uint32_t* index, int64_t n_fluid,
+                     int64_t n_cells, void* stream) {
+    SparseArgs a;
+    int rc = sparse_common(p, src, dst, n_fluid, n_cells, a);
+    if (rc) return rc;
+    if (src == dst) return fail(LBM_E_INVALID, "the sparse sweep needs two distinct PDF lists");
+    if ((rc = check_device_ptr(p, index, "index", false))) return rc;
+    a.index = index;
+    SparseLauncher L = sparse_launcher(p);
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no sparse kernel built for this stencil/method/dtype");
+    if (n_fluid == 0) return LBM_OK;
+    cudaError_t e = L(a, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "sparse sweep launch");
+}
+
+int lbm_sparse_set_equilibrium(const LbmPlan* p, void* pdfs, const double* rho, const double* u, int64_t n_fluid,
+                               int64_t n_cells, void* stream) {
+    SparseArgs a;
+    int rc = sparse_common(p, pdfs, pdfs, n_fluid, n_cells, a);
+    if (rc) return rc;
+    if ((rc = check_device_ptr(p, rho, "rho", false))) return rc;
+    if ((rc = check_device_ptr(p, u, "u", false))) return rc;
+    SparseSetLauncher L = sparse_set_launcher(p);
+    if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no sparse setter kernel");
+    if (n_fluid == 0) return LBM_OK;
+    cudaError_t e = L(a, rho, u, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "sparse setter launch");
+}
+
+int lbm_sparse_get_macroscopic(const LbmPlan* p, const void* pdfs, double* rho, double* u, int64_t n_fluid,
+                               int64_t n_cells, void* stream) {
+    SparseArgs a;
+    int rc = sparse_common(p, pdfs, pdfs, n_fluid, n_cells, a);
+    if (rc) return rc;
+    if ((rc = check_device_ptr(p, rho, "rho", true))) return rc;
+    if ((rc = check_device_ptr(p, u, "u", true))) return rc;
+    if (n_fluid == 0) return LBM_OK;
+    cudaError_t e;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (p->q == 19)
+        e = p->store == ST_F64 ? launch_sparse_get<double, double, 19>(a, rho, u, s)
+                               : launch_sparse_get<float, float, 19>(a, rho, u, s);
+    else
+        e = p->store == ST_F64 ? launch_sparse_get<double, double, 27>(a, rho, u, s)
+                               : launch_sparse_get<float, float, 27>(a, rho, u, s);
+    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "sparse getter launch");
+}
+
+int lbm_sparse_ubb(const LbmPlan* p, void* pdfs, const uint32_t* links, int64_t n_links, int64_t n_cells,
+                   const double velocity[3], void* stream) {
+    SparseArgs a;
+    int rc = sparse_common(p, pdfs, pdfs, 0, n_cells, a);
+    if (rc) return rc;
+    if (velocity == nullptr) return fail(LBM_E_INVALID, "velocity must not be NULL");
+    if (n_links < 0 || n_links / 256 >= (int64_t)INT32_MAX) return fail(LBM_E_INVALID, "bad number of links");
+    if (n_links == 0) return LBM_OK;
+    if ((rc = check_device_ptr(p, links, "links", false))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    if (p->q == 19)
+        e = p->store == ST_F64 ? launch_sparse_ubb<double, double, 19>(a, links, n_links, velocity, s)
+                               : launch_sparse_ubb<float, float, 19>(a, links, n_links, velocity, s);
+    else
+        e = p->store == ST_F64 ? launch_sparse_ubb<double, double, 27>(a, links, n_links, velocity, s)
+                               : launch_sparse_ubb<float, float, 27>(a, links, n_links, velocity, s);
+    return e == cudaSuccess ? LBM_OK : cuda_fail(e, "sparse UBB launch");
+}
+
+}  // extern "C"
+
 // ---------------------------------------------------------------------------------------------
 // Batched domains: one persistent launch per step over a tile table spanning every domain.
 
@@ -970,6 +1185,7 @@ BatchLauncher batched_launcher(int q, int mk, int store, int pat) {
     if (q == 27 && mk == MK_MRT) return batched_q27_mrt(store, pat);
     if (q == 27 && mk == MK_CUM) return batched_q27_cum(store, pat);
     if (q == 27 && mk == MK_CUM1) return batched_q27_cum1(store, pat);
+    if (q == 27 && mk == MK_CM) return batched_q27_cm(store, pat);
     return nullptr;
 }
 
@@ -1025,8 +1241,10 @@ int lbm_batch_create(const LbmPlanDesc* common, const LbmDomainDesc* domains, in
                     t.tile_x, t.tile_y, t.cells_z, t.blocks_per_sm);
     if (common->pattern != LBM_PATTERN_PULL && common->pattern != LBM_PATTERN_AA)
         return fail(LBM_E_UNSUPPORTED, "batched sweeps are built for the pull and AA patterns");
-    if (common->fixed_density != 0.0)
+    if (common->fixed_density != 0.0 || common->fixed_density1 != 0.0)
         return fail(LBM_E_UNSUPPORTED, "batched sweeps are built without FixedDensity boundaries");
+    if (common->fourth_order_limiter != 0.0)
+        return fail(LBM_E_UNSUPPORTED, "batched sweeps are built without the fourth-order correction");
     const bool inplace = common->pattern != LBM_PATTERN_PULL;
     if (inplace && buffer_b == nullptr) buffer_b = buffer_a;
     if (inplace && buffer_b != buffer_a) return fail(LBM_E_INVALID, "in-place patterns use buffer_a only");
@@ -1076,7 +1294,9 @@ int lbm_batch_create(const LbmPlanDesc* common, const LbmDomainDesc* domains, in
 
     const int q = common->stencil;
     if (common->sgs == LBM_SGS_MLP) return fail(LBM_E_UNSUPPORTED, "batched sweeps do not take the learned closure");
-    int mk = common->method == LBM_METHOD_MRT ? MK_MRT : (common->method == LBM_METHOD_CUMULANT ? MK_CUM : MK_POP);
+    int mk = common->method == LBM_METHOD_MRT ? MK_MRT
+             : common->method == LBM_METHOD_CUMULANT ? MK_CUM
+             : common->method == LBM_METHOD_CENTRAL_MOMENT ? MK_CM : MK_POP;
     if (mk == MK_CUM && all_cum1) mk = MK_CUM1;
     const int store = common->store_dtype;
     if (batched_launcher(q, mk, store, PAT_PULL) == nullptr)

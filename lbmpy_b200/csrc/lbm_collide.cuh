@@ -169,12 +169,33 @@ __device__ __forceinline__ R collide_mrt(R (&f)[Q], const Physics& p) {
                                                 : R(L::w(i)) * (R(9) * cF * cu + R(3) * cF - R(3) * uF);
         }
     }
+    // Every row of the weighted-orthogonal basis is even or odd under c -> -c, so the transforms
+    // run on the sums and differences of opposite populations, f_i +- f_inv(i): half the terms
+    // of the dense Q x Q products.
+    constexpr int NP = (Q - 1) / 2;
+    R fs[NP], fd[NP], ls[NP], ld[NP];
+#pragma unroll
+    for (int p2 = 0; p2 < NP; ++p2) {
+        const int i = L::pair(p2), j = L::inv(L::pair(p2));
+        fs[p2] = f[i] + f[j];
+        fd[p2] = f[i] - f[j];
+        if (has_force) {
+            ls[p2] = luo[i] + luo[j];
+            ld[p2] = luo[i] - luo[j];
+        }
+    }
     R delta[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         R mk = 0;
+        if (L::Meven(k)) {
+            mk = cmad(mk, L::M(k, 0), f[0]);
 #pragma unroll
-        for (int i = 0; i < Q; ++i) mk = cmad(mk, L::M(k, i), f[i]);
+            for (int p2 = 0; p2 < NP; ++p2) mk = cmad(mk, L::M(k, L::pair(p2)), fs[p2]);
+        } else {
+#pragma unroll
+            for (int p2 = 0; p2 < NP; ++p2) mk = cmad(mk, L::M(k, L::pair(p2)), fd[p2]);
+        }
         R lin = 0, quad = 0;
         lin = cmad(lin, L::mlin(k, 0), m.ux);
         lin = cmad(lin, L::mlin(k, 1), m.uy);
@@ -187,19 +208,39 @@ __device__ __forceinline__ R collide_mrt(R (&f)[Q], const Physics& p) {
         R d = r * (meq - mk);
         if (has_force) {
             R fk = 0;
+            if (L::Meven(k)) {
+                fk = cmad(fk, L::M(k, 0), luo[0]);
 #pragma unroll
-            for (int i = 0; i < Q; ++i) fk = cmad(fk, L::M(k, i), luo[i]);
+                for (int p2 = 0; p2 < NP; ++p2) fk = cmad(fk, L::M(k, L::pair(p2)), ls[p2]);
+            } else {
+#pragma unroll
+                for (int p2 = 0; p2 < NP; ++p2) fk = cmad(fk, L::M(k, L::pair(p2)), ld[p2]);
+            }
             if (p.force_model == FM_GUO) fk *= (R(1) - R(0.5) * r);
             d += fk;
         }
         delta[k] = d;
     }
+    // back: column k of M^-1 is even or odd with row k of M, so f_i and f_inv(i) receive the even
+    // part plus or minus the odd part
+    {
+        R e0 = 0;
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        R s = 0;
+        for (int k = 0; k < Q; ++k)
+            if (L::Meven(k)) e0 = cmad(e0, L::Minv(0, k), delta[k]);
+        f[0] += e0;
+    }
 #pragma unroll
-        for (int k = 0; k < Q; ++k) s = cmad(s, L::Minv(i, k), delta[k]);
-        f[i] += s;
+    for (int p2 = 0; p2 < NP; ++p2) {
+        const int i = L::pair(p2);
+        R e = 0, o = 0;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            if (L::Meven(k)) e = cmad(e, L::Minv(i, k), delta[k]);
+            else o = cmad(o, L::Minv(i, k), delta[k]);
+        }
+        f[i] += e + o;
+        f[L::inv(i)] += e - o;
     }
     return p.sgs == 1 ? om_sgs : R(0);
 }
@@ -331,22 +372,52 @@ __device__ __forceinline__ R collide_cum(R (&f)[27], const Physics& p) {
     const R c020 = c200 - Ps_d1;
     const R c002 = c200 - Ps_d2;
     // third order: sums and differences relax separately, xyz alone
-    const R s1 = (k120 + k102) * (R(1) - rate(10)), s2 = (k210 + k012) * (R(1) - rate(11)),
-            s3 = (k201 + k021) * (R(1) - rate(12));
-    const R d1 = (k120 - k102) * (R(1) - rate(13)), d2 = (k210 - k012) * (R(1) - rate(14)),
-            d3 = (k201 - k021) * (R(1) - rate(15));
-    const R c111 = k111 * (R(1) - rate(16));
+    R w_s[3] = {rate(10), rate(11), rate(12)}, w_d[3] = {rate(13), rate(14), rate(15)}, w_xyz = rate(16);
+    if (p.foc_limiter > 0.0) {
+        // fourth-order correction: the optimal third-order rates of the plan, limited per cell by
+        // the magnitude of the x-variant cumulant of each group (fourth_order_correction.py:199-211)
+        const R lim = R(p.foc_limiter) * rho;
+        const R a3 = fabs(k120 + k102), a4 = fabs(k120 - k102), a5 = fabs(k111);
+        const R l3 = w_s[0] + (R(1) - w_s[0]) * a3 / (lim + a3);
+        const R l4 = w_d[0] + (R(1) - w_d[0]) * a4 / (lim + a4);
+        w_s[0] = w_s[1] = w_s[2] = l3;
+        w_d[0] = w_d[1] = w_d[2] = l4;
+        w_xyz = w_xyz + (R(1) - w_xyz) * a5 / (lim + a5);
+    }
+    const R s1 = (k120 + k102) * (R(1) - w_s[0]), s2 = (k210 + k012) * (R(1) - w_s[1]),
+            s3 = (k201 + k021) * (R(1) - w_s[2]);
+    const R d1 = (k120 - k102) * (R(1) - w_d[0]), d2 = (k210 - k012) * (R(1) - w_d[1]),
+            d3 = (k201 - k021) * (R(1) - w_d[2]);
+    const R c111 = k111 * (R(1) - w_xyz);
     const R c120 = R(0.5) * (s1 + d1), c102 = R(0.5) * (s1 - d1);
     const R c210 = R(0.5) * (s2 + d2), c012 = R(0.5) * (s2 - d2);
     const R c201 = R(0.5) * (s3 + d3), c021 = R(0.5) * (s3 - d3);
     // fourth order
-    const R q1 = (C220 - R(2) * C202 + C022) * (R(1) - rate(17));
-    const R q2 = (C220 + C202 - R(2) * C022) * (R(1) - rate(18));
-    const R q3 = (C220 + C202 + C022) * (R(1) - rate(19));
+    R q1 = (C220 - R(2) * C202 + C022) * (R(1) - rate(17));
+    R q2 = (C220 + C202 - R(2) * C022) * (R(1) - rate(18));
+    R q3 = (C220 + C202 + C022) * (R(1) - rate(19));
+    R C211s = C211 * (R(1) - rate(20)), C121s = C121 * (R(1) - rate(21)), C112s = C112 * (R(1) - rate(22));
+    if (p.foc_limiter > 0.0) {
+        // correction terms of the fourth-order polynomial cumulants from velocity-derivative
+        // estimates of the pre-collision second-order cumulants (Geier et al. 2017, eq. 44-49;
+        // fourth_order_correction.py:100-145)
+        const R o1 = R(p.rates[4]), o2 = R(p.rates[9]);
+        const R h = R(0.5) * irho;
+        const R Dx = -o1 * h * (R(2) * k200 - k020 - k002) - o2 * h * (k200 + k020 + k002 - rho);
+        const R Dy = Dx + R(3) * o1 * h * (k200 - k020);
+        const R Dz = Dx + R(3) * o1 * h * (k200 - k002);
+        const R g = (R(1) / o1 - R(0.5)) * rho;
+        const R ca = g * R(p.foc_a), cb = g * R(p.foc_b) * R(-1.0 / 3.0) * R(-3) * o1 * irho;
+        q1 += R(2.0 / 3.0) * R(p.rates[17]) * ca * (Dx - R(2) * Dy + Dz);
+        q2 += R(2.0 / 3.0) * R(p.rates[17]) * ca * (Dx + Dy - R(2) * Dz);
+        q3 += R(-4.0 / 3.0) * R(p.rates[19]) * ca * (Dx + Dy + Dz);
+        C211s += R(p.rates[20]) * cb * k011;
+        C121s += R(p.rates[20]) * cb * k101;
+        C112s += R(p.rates[20]) * cb * k110;
+    }
     const R C220s = (q3 + q1 + q2) * R(1.0 / 3.0);
     const R C202s = (q3 - q1) * R(1.0 / 3.0);
     const R C022s = (q3 - q2) * R(1.0 / 3.0);
-    const R C211s = C211 * (R(1) - rate(20)), C121s = C121 * (R(1) - rate(21)), C112s = C112 * (R(1) - rate(22));
     const R C221s = C221 * (R(1) - rate(23)), C212s = C212 * (R(1) - rate(24)), C122s = C122 * (R(1) - rate(25));
     const R C222s = C222 * (R(1) - rate(26));
 
@@ -393,6 +464,121 @@ __device__ __forceinline__ R collide_cum(R (&f)[27], const Physics& p) {
 #pragma unroll
     for (int i = 0; i < 27; ++i) f[i] = k[cube<27>(i)];
     return p.sgs == 1 ? om_sgs : R(p.rates[4]);
+}
+
+// D3Q27 central-moment method (methods/momentbased/centralmomentbasedmethod.py:296-394): the
+// polynomial central moments of the method's groups (the cumulant groups, default_moment_sets.py:
+// 110-148) about the equilibrium velocity relax towards rho times the central moments of a
+// Gaussian of variance 1/3; the force model's population term (Simple, Luo, Guo) enters in
+// central-moment space, scaled by (1 - omega/2) per moment for Guo (forcemodels.py:201-203,
+// 261-263, 300-306).  Compressible, zero-centred storage with the lattice-weight background.
+template <class R>
+__device__ __forceinline__ R collide_cm(R (&f)[27], const Physics& p) {
+    using L = Lat<27>;
+    const bool guo = p.force_model == FM_GUO;
+    const bool forced = p.force_model == FM_GUO || p.force_model == FM_LUO || p.force_model == FM_SIMPLE;
+    const Macro<27, R> m = conserved<27, R>(f, p, guo);   // Guo: equilibrium velocity shift F / (2 rho)
+    const R rho = m.rho;
+    const R ux = m.ux, uy = m.uy, uz = m.uz;
+    R k[27];
+#pragma unroll
+    for (int i = 0; i < 27; ++i) k[cube<27>(i)] = f[i];
+    chimera_forward(k, uz, 1, 9, 3);
+    chimera_forward(k, uy, 3, 9, 1);
+    chimera_forward(k, ux, 9, 3, 1);
+    const R bx[3] = {R(1), -ux, R(1.0 / 3.0) + ux * ux};
+    const R by[3] = {R(1), -uy, R(1.0 / 3.0) + uy * uy};
+    const R bz[3] = {R(1), -uz, R(1.0 / 3.0) + uz * uz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) k[a * 9 + b * 3 + c] += bx[a] * by[b] * bz[c];
+    // central moments of the force model's population term about the same velocity
+    R g[27];
+#pragma unroll
+    for (int i = 0; i < 27; ++i) g[i] = R(0);
+    if (forced) {
+        const R Fx = R(p.force[0]), Fy = R(p.force[1]), Fz = R(p.force[2]);
+#pragma unroll
+        for (int i = 0; i < 27; ++i) {
+            const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
+            const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
+            const R uF = ux * Fx + uy * Fy + uz * Fz;
+            g[cube<27>(i)] = p.force_model == FM_SIMPLE ? R(L::w(i)) * R(3) * cF
+                                                        : R(L::w(i)) * (R(3) * (cF - uF) + R(9) * cu * cF);
+        }
+        chimera_forward(g, uz, 1, 9, 3);
+        chimera_forward(g, uy, 3, 9, 1);
+        chimera_forward(g, ux, 9, 3, 1);
+    }
+#define K(a, b, c) k[(a) * 9 + (b) * 3 + (c)]
+#define G(a, b, c) g[(a) * 9 + (b) * 3 + (c)]
+    // post = pre + omega (eq - pre) + corr * force, corr = 1 - omega/2 for Guo
+    auto relax = [&](int idx, R pre, R eq, R frc) -> R {
+        const R w = R(p.rates[idx]);
+        return pre + w * (eq - pre) + (guo ? R(1) - R(0.5) * w : R(1)) * frc;
+    };
+    const R third = R(1.0 / 3.0);
+    // first order: conserved (rate 0); the force term alone changes them
+    const R p100 = K(1, 0, 0) + G(1, 0, 0), p010 = K(0, 1, 0) + G(0, 1, 0), p001 = K(0, 0, 1) + G(0, 0, 1);
+    // second order
+    const R c110 = relax(4, K(1, 1, 0), R(0), G(1, 1, 0));
+    const R c101 = relax(5, K(1, 0, 1), R(0), G(1, 0, 1));
+    const R c011 = relax(6, K(0, 1, 1), R(0), G(0, 1, 1));
+    const R D1 = relax(7, K(2, 0, 0) - K(0, 2, 0), R(0), G(2, 0, 0) - G(0, 2, 0));
+    const R D2 = relax(8, K(2, 0, 0) - K(0, 0, 2), R(0), G(2, 0, 0) - G(0, 0, 2));
+    const R Sb = relax(9, K(2, 0, 0) + K(0, 2, 0) + K(0, 0, 2), rho, G(2, 0, 0) + G(0, 2, 0) + G(0, 0, 2));
+    const R c200 = (Sb + D1 + D2) * third, c020 = c200 - D1, c002 = c200 - D2;
+    // third order: sums and differences, xyz
+    const R s1 = relax(10, K(1, 2, 0) + K(1, 0, 2), R(0), G(1, 2, 0) + G(1, 0, 2));
+    const R s2 = relax(11, K(2, 1, 0) + K(0, 1, 2), R(0), G(2, 1, 0) + G(0, 1, 2));
+    const R s3 = relax(12, K(2, 0, 1) + K(0, 2, 1), R(0), G(2, 0, 1) + G(0, 2, 1));
+    const R d1 = relax(13, K(1, 2, 0) - K(1, 0, 2), R(0), G(1, 2, 0) - G(1, 0, 2));
+    const R d2 = relax(14, K(2, 1, 0) - K(0, 1, 2), R(0), G(2, 1, 0) - G(0, 1, 2));
+    const R d3 = relax(15, K(2, 0, 1) - K(0, 2, 1), R(0), G(2, 0, 1) - G(0, 2, 1));
+    const R c111 = relax(16, K(1, 1, 1), R(0), G(1, 1, 1));
+    // fourth order
+    const R q1 = relax(17, K(2, 2, 0) - R(2) * K(2, 0, 2) + K(0, 2, 2), R(0),
+                       G(2, 2, 0) - R(2) * G(2, 0, 2) + G(0, 2, 2));
+    const R q2 = relax(18, K(2, 2, 0) + K(2, 0, 2) - R(2) * K(0, 2, 2), R(0),
+                       G(2, 2, 0) + G(2, 0, 2) - R(2) * G(0, 2, 2));
+    const R q3 = relax(19, K(2, 2, 0) + K(2, 0, 2) + K(0, 2, 2), rho * third, G(2, 2, 0) + G(2, 0, 2) + G(0, 2, 2));
+    const R c211 = relax(20, K(2, 1, 1), R(0), G(2, 1, 1));
+    const R c121 = relax(21, K(1, 2, 1), R(0), G(1, 2, 1));
+    const R c112 = relax(22, K(1, 1, 2), R(0), G(1, 1, 2));
+    // fifth and sixth order
+    const R c221 = relax(23, K(2, 2, 1), R(0), G(2, 2, 1));
+    const R c212 = relax(24, K(2, 1, 2), R(0), G(2, 1, 2));
+    const R c122 = relax(25, K(1, 2, 2), R(0), G(1, 2, 2));
+    const R c222 = relax(26, K(2, 2, 2), rho * R(1.0 / 27.0), G(2, 2, 2));
+    K(0, 0, 0) = rho;
+    K(1, 0, 0) = p100; K(0, 1, 0) = p010; K(0, 0, 1) = p001;
+    K(1, 1, 0) = c110; K(1, 0, 1) = c101; K(0, 1, 1) = c011;
+    K(2, 0, 0) = c200; K(0, 2, 0) = c020; K(0, 0, 2) = c002;
+    K(1, 2, 0) = R(0.5) * (s1 + d1); K(1, 0, 2) = R(0.5) * (s1 - d1);
+    K(2, 1, 0) = R(0.5) * (s2 + d2); K(0, 1, 2) = R(0.5) * (s2 - d2);
+    K(2, 0, 1) = R(0.5) * (s3 + d3); K(0, 2, 1) = R(0.5) * (s3 - d3);
+    K(1, 1, 1) = c111;
+    K(2, 2, 0) = (q3 + q1 + q2) * third; K(2, 0, 2) = (q3 - q1) * third; K(0, 2, 2) = (q3 - q2) * third;
+    K(2, 1, 1) = c211; K(1, 2, 1) = c121; K(1, 1, 2) = c112;
+    K(2, 2, 1) = c221; K(2, 1, 2) = c212; K(1, 2, 2) = c122;
+    K(2, 2, 2) = c222;
+#undef K
+#undef G
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) k[a * 9 + b * 3 + c] -= bx[a] * by[b] * bz[c];
+    chimera_backward(k, ux, 9, 3, 1);
+    chimera_backward(k, uy, 3, 9, 1);
+    chimera_backward(k, uz, 1, 9, 3);
+#pragma unroll
+    for (int i = 0; i < 27; ++i) f[i] = k[cube<27>(i)];
+    return R(p.rates[4]);
 }
 
 // D3Q27 cumulant when every cumulant of third and higher order relaxes with rate 1 (lbmpy's
@@ -553,7 +739,7 @@ template <int Q, class R, int MK>
 __device__ __forceinline__ void equilibrium(R (&f)[Q], R rho, R ux, R uy, R uz, const Physics& p) {
     using L = Lat<Q>;
     const R drho = rho - R(1);
-    if (MK == MK_CUM) {
+    if (MK == MK_CUM || MK == MK_CM) {
         // product form: kappa = rho * Gaussian moments (variance 1/3), shifted by u
         const R phx[3] = {R(0.5) * (R(1.0 / 3.0) + ux * ux - ux), R(2.0 / 3.0) - ux * ux,
                           R(0.5) * (R(1.0 / 3.0) + ux * ux + ux)};

@@ -9,9 +9,10 @@
 
 namespace lbm {
 
-enum StoreType : int { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3 };
-// SRT/TRT | raw-moment MRT | cumulant | cumulant with every order >= 3 relaxed by 1
-enum MethodKind : int { MK_POP = 0, MK_MRT = 1, MK_CUM = 2, MK_CUM1 = 3, MK_CUM1_MLP = 4 };
+enum StoreType : int { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3, ST_E3M12 = 4 };
+// SRT/TRT | raw-moment MRT | cumulant | cumulant with every order >= 3 relaxed by 1 | with a learned
+// closure | D3Q27 central moments
+enum MethodKind : int { MK_POP = 0, MK_MRT = 1, MK_CUM = 2, MK_CUM1 = 3, MK_CUM1_MLP = 4, MK_CM = 5 };
 enum PatternKind : int {
     PAT_PULL = 0, PAT_AA_EVEN = 1, PAT_AA_ODD = 2, PAT_ESO_EVEN = 3, PAT_ESO_ODD = 4,
     PAT_PUSH = 5, PAT_EPULL_EVEN = 6, PAT_EPULL_ODD = 7, PAT_EPUSH_EVEN = 8, PAT_EPUSH_ODD = 9
@@ -63,6 +64,7 @@ template <> struct Lat<19> {
     LBM_HD static constexpr int cy(int i) { return lbm_tables::q19_cy(i); }
     LBM_HD static constexpr int cz(int i) { return lbm_tables::q19_cz(i); }
     LBM_HD static constexpr int inv(int i) { return lbm_tables::q19_inv(i); }
+    LBM_HD static constexpr int pair(int p) { return lbm_tables::q19_pair(p); }   // p < (Q - 1) / 2
     LBM_HD static constexpr double w(int i) { return lbm_tables::q19_w(i); }
     LBM_HD static constexpr double eqlin(bool cont, int i, int a) {
         return cont ? lbm_tables::q19_eqlin_cont(i, a) : lbm_tables::q19_eqlin_disc(i, a);
@@ -71,6 +73,7 @@ template <> struct Lat<19> {
         return cont ? lbm_tables::q19_eqquad_cont(i, a) : lbm_tables::q19_eqquad_disc(i, a);
     }
     LBM_HD static constexpr double M(int k, int i) { return lbm_tables::q19_mrt_M(k, i); }
+    LBM_HD static constexpr bool Meven(int k) { return lbm_tables::q19_mrt_even(k) != 0; }
     LBM_HD static constexpr double Minv(int i, int k) { return lbm_tables::q19_mrt_Minv(i, k); }
     LBM_HD static constexpr double p0(int k) { return lbm_tables::q19_mrt_p0(k); }
     LBM_HD static constexpr double mlin(int k, int a) { return lbm_tables::q19_mrt_lin(k, a); }
@@ -83,6 +86,7 @@ template <> struct Lat<27> {
     LBM_HD static constexpr int cy(int i) { return lbm_tables::q27_cy(i); }
     LBM_HD static constexpr int cz(int i) { return lbm_tables::q27_cz(i); }
     LBM_HD static constexpr int inv(int i) { return lbm_tables::q27_inv(i); }
+    LBM_HD static constexpr int pair(int p) { return lbm_tables::q27_pair(p); }   // p < (Q - 1) / 2
     LBM_HD static constexpr double w(int i) { return lbm_tables::q27_w(i); }
     LBM_HD static constexpr double eqlin(bool cont, int i, int a) {
         return cont ? lbm_tables::q27_eqlin_cont(i, a) : lbm_tables::q27_eqlin_disc(i, a);
@@ -91,6 +95,7 @@ template <> struct Lat<27> {
         return cont ? lbm_tables::q27_eqquad_cont(i, a) : lbm_tables::q27_eqquad_disc(i, a);
     }
     LBM_HD static constexpr double M(int k, int i) { return lbm_tables::q27_mrt_M(k, i); }
+    LBM_HD static constexpr bool Meven(int k) { return lbm_tables::q27_mrt_even(k) != 0; }
     LBM_HD static constexpr double Minv(int i, int k) { return lbm_tables::q27_mrt_Minv(i, k); }
     LBM_HD static constexpr double p0(int k) { return lbm_tables::q27_mrt_p0(k); }
     LBM_HD static constexpr double mlin(int k, int a) { return lbm_tables::q27_mrt_lin(k, a); }
@@ -116,6 +121,36 @@ template <class R> struct Conv<__nv_bfloat16, R> {
     __device__ __forceinline__ static void st(__nv_bfloat16* p, R v) { *p = __float2bfloat16_rn((float)v); }
 };
 
+// e3m12: a 16-bit float for zero-centred PDFs, which stay far below 1 in magnitude: sign, 3 exponent
+// bits and 12 mantissa bits, scaled by 16.  Code (s, E, M) holds (-1)^s (1 + M/4096) 2^(E-12) for
+// E = 1..7 and (-1)^s M 2^-23 for E = 0 (gradual underflow), so |value| < 1/16 with a relative step
+// of 2^-12 (IEEE half: 2^-10) down to 2^-11, and an absolute step of 2^-23 below.  Larger
+// magnitudes saturate.  The bits are those of the FP32 number value * 2^-115 shifted right by 11:
+// decoding is an integer shift and one FP32 multiply (the FP32 subnormal range carries E = 0),
+// encoding one multiply, rounding to nearest even on the dropped 11 bits, and a clamp.
+struct e3m12 {
+    uint16_t bits;
+};
+
+#ifdef __CUDACC__   // device intrinsics; host-only builds of the collision code do not store e3m12
+__device__ __forceinline__ float e3m12_decode(unsigned h) {
+    const unsigned b = ((h & 0x7fffu) << 11) | ((h & 0x8000u) << 16);
+    return __fmul_rn(__uint_as_float(b), 0x1p115f);
+}
+
+__device__ __forceinline__ unsigned e3m12_encode(float v) {
+    const unsigned b = __float_as_uint(__fmul_rn(v, 0x1p-115f));
+    const unsigned mag = b & 0x7fffffffu;
+    const unsigned c = min((mag + 0x3ffu + ((mag >> 11) & 1u)) >> 11, 0x7fffu);
+    return c | ((b >> 16) & 0x8000u);
+}
+
+template <class R> struct Conv<e3m12, R> {
+    __device__ __forceinline__ static R ld(const e3m12* p) { return (R)e3m12_decode(p->bits); }
+    __device__ __forceinline__ static void st(e3m12* p, R v) { p->bits = (uint16_t)e3m12_encode((float)v); }
+};
+#endif
+
 // ------------------------------------------------------------------ kernel arguments
 struct Physics {
     double rates[27];      // per moment (MRT), per polynomial cumulant, or [omega+, omega-] (SRT/TRT)
@@ -134,6 +169,8 @@ struct Physics {
     double ubb_density[MAX_UBB];  // prescribed wall density of UBB number u (0: the fluid cell's density)
     unsigned ubb_link_mask;       // bit u: UBB number u takes per-link velocities (SweepArgs::ubb_link_vel)
     unsigned ubb_adapt_mask;      // bit u: the wall velocity is shifted by -F / (2 rho_ref)
+    double foc_limiter;           // > 0: fourth-order cumulant correction with this limiter
+    double foc_a, foc_b;          // its parameters a and b (Geier et al. 2017, eq. 115-116)
 };
 
 struct Grid {
@@ -156,7 +193,9 @@ struct SweepArgs {
     void* dst;
     float* omega_out;      // optional per-cell effective shear rate (interior, x fastest)
     int zc;                // closure sweep: consecutive z-planes per thread (next plane prefetched to L2)
-    int pad_;
+    int stage_probe;       // staged sweep: before its last tile each CTA also waits on a barrier that
+                           // nothing arrives at (exercises the bounded wait and the status report)
+    unsigned long long stage_wait_ns;   // staged sweep: bound of each barrier wait (0: 1 s)
     const void* ubb_rho;   // compressible moving walls: previous-step density of the cells next to them
     unsigned* status;      // device status word of the plan (STATUS_* bits), or nullptr
     // Per-link boundary data: block index of each interior cell (x fastest, -1: none) and, per

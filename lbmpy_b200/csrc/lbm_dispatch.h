@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <type_traits>
 
 #include "lbm_quad.cuh"
 #include "lbm_staged.cuh"
@@ -100,6 +101,23 @@ StagedLauncher pick_staged_pattern(int pat) {
     return nullptr;
 }
 
+using SparseLauncher = cudaError_t (*)(const SparseArgs&, cudaStream_t);
+using SparseSetLauncher = cudaError_t (*)(const SparseArgs&, const double*, const double*, cudaStream_t);
+
+template <class S, class R, int Q, int MK>
+cudaError_t launch_sparse(const SparseArgs& a, cudaStream_t s) {
+    const long long blocks = (a.n_fluid + 255) / 256;
+    k_sweep_sparse<S, R, Q, MK><<<(unsigned)blocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S, class R, int Q, int MK>
+cudaError_t launch_sparse_set(const SparseArgs& a, const double* rho, const double* u, cudaStream_t s) {
+    const long long blocks = (a.n_fluid + 255) / 256;
+    k_sparse_set_equilibrium<S, R, Q, MK><<<(unsigned)blocks, 256, 0, s>>>(a, rho, u);
+    return cudaGetLastError();
+}
+
 using BatchLauncher = cudaError_t (*)(const BatchArgs&, dim3, dim3, cudaStream_t);
 
 template <class S, class R, int Q, int MK, int PAT>
@@ -124,46 +142,58 @@ SweepLauncher pick_sweep_pattern(int pat) {
         case PAT_PULL: return &launch_sweep<S, R, Q, MK, PAT_PULL>;
         case PAT_AA_EVEN: return &launch_sweep<S, R, Q, MK, PAT_AA_EVEN>;
         case PAT_AA_ODD: return &launch_sweep<S, R, Q, MK, PAT_AA_ODD>;
-        case PAT_ESO_EVEN: return &launch_sweep<S, R, Q, MK, PAT_ESO_EVEN>;
-        case PAT_ESO_ODD: return &launch_sweep<S, R, Q, MK, PAT_ESO_ODD>;
     }
-    if constexpr (sizeof(S) >= 4) {
+    if constexpr (std::is_same<S, e3m12>::value) {
+        return nullptr;   // e3m12: pull and AA
+    } else {
         switch (pat) {
-            case PAT_PUSH: return &launch_sweep<S, R, Q, MK, PAT_PUSH>;
-            case PAT_EPULL_EVEN: return &launch_sweep<S, R, Q, MK, PAT_EPULL_EVEN>;
-            case PAT_EPULL_ODD: return &launch_sweep<S, R, Q, MK, PAT_EPULL_ODD>;
-            case PAT_EPUSH_EVEN: return &launch_sweep<S, R, Q, MK, PAT_EPUSH_EVEN>;
-            case PAT_EPUSH_ODD: return &launch_sweep<S, R, Q, MK, PAT_EPUSH_ODD>;
+            case PAT_ESO_EVEN: return &launch_sweep<S, R, Q, MK, PAT_ESO_EVEN>;
+            case PAT_ESO_ODD: return &launch_sweep<S, R, Q, MK, PAT_ESO_ODD>;
         }
+        if constexpr (sizeof(S) >= 4) {
+            switch (pat) {
+                case PAT_PUSH: return &launch_sweep<S, R, Q, MK, PAT_PUSH>;
+                case PAT_EPULL_EVEN: return &launch_sweep<S, R, Q, MK, PAT_EPULL_EVEN>;
+                case PAT_EPULL_ODD: return &launch_sweep<S, R, Q, MK, PAT_EPULL_ODD>;
+                case PAT_EPUSH_EVEN: return &launch_sweep<S, R, Q, MK, PAT_EPUSH_EVEN>;
+                case PAT_EPUSH_ODD: return &launch_sweep<S, R, Q, MK, PAT_EPUSH_ODD>;
+            }
+        }
+        return nullptr;
     }
-    return nullptr;
 }
 
 template <class S, class R, int Q, int MK, int PAT>
-cudaError_t launch_fixed_density(const SweepArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
-    k_fixed_density<S, R, Q, MK, PAT><<<grid, block, 0, s>>>(a);
+cudaError_t launch_prepass(const SweepArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
+    k_boundary_prepass<S, R, Q, MK, PAT><<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
 
 template <class S, class R, int Q, int MK>
-SweepLauncher pick_fixed_density_pattern(int pat) {
+SweepLauncher pick_prepass_pattern(int pat) {
     switch (pat) {
-        case PAT_PULL: return &launch_fixed_density<S, R, Q, MK, PAT_PULL>;
-        case PAT_AA_EVEN: return &launch_fixed_density<S, R, Q, MK, PAT_AA_EVEN>;
-        case PAT_AA_ODD: return &launch_fixed_density<S, R, Q, MK, PAT_AA_ODD>;
-        case PAT_ESO_EVEN: return &launch_fixed_density<S, R, Q, MK, PAT_ESO_EVEN>;
-        case PAT_ESO_ODD: return &launch_fixed_density<S, R, Q, MK, PAT_ESO_ODD>;
+        case PAT_PULL: return &launch_prepass<S, R, Q, MK, PAT_PULL>;
+        case PAT_AA_EVEN: return &launch_prepass<S, R, Q, MK, PAT_AA_EVEN>;
+        case PAT_AA_ODD: return &launch_prepass<S, R, Q, MK, PAT_AA_ODD>;
     }
-    if constexpr (sizeof(S) >= 4) {
+    if constexpr (std::is_same<S, e3m12>::value) {
+        return nullptr;   // e3m12: pull and AA
+    } else {
         switch (pat) {
-            case PAT_PUSH: return &launch_fixed_density<S, R, Q, MK, PAT_PUSH>;
-            case PAT_EPULL_EVEN: return &launch_fixed_density<S, R, Q, MK, PAT_EPULL_EVEN>;
-            case PAT_EPULL_ODD: return &launch_fixed_density<S, R, Q, MK, PAT_EPULL_ODD>;
-            case PAT_EPUSH_EVEN: return &launch_fixed_density<S, R, Q, MK, PAT_EPUSH_EVEN>;
-            case PAT_EPUSH_ODD: return &launch_fixed_density<S, R, Q, MK, PAT_EPUSH_ODD>;
+            case PAT_ESO_EVEN: return &launch_prepass<S, R, Q, MK, PAT_ESO_EVEN>;
+            case PAT_ESO_ODD: return &launch_prepass<S, R, Q, MK, PAT_ESO_ODD>;
         }
+        if constexpr (sizeof(S) >= 4) {
+            switch (pat) {
+                case PAT_PUSH: return &launch_prepass<S, R, Q, MK, PAT_PUSH>;
+                case PAT_EPULL_EVEN: return &launch_prepass<S, R, Q, MK, PAT_EPULL_EVEN>;
+                case PAT_EPULL_ODD: return &launch_prepass<S, R, Q, MK, PAT_EPULL_ODD>;
+                case PAT_EPUSH_EVEN: return &launch_prepass<S, R, Q, MK, PAT_EPUSH_EVEN>;
+                case PAT_EPUSH_ODD: return &launch_prepass<S, R, Q, MK, PAT_EPUSH_ODD>;
+            }
+        }
+        return nullptr;
     }
-    return nullptr;
 }
 
 template <class S, class R, int Q, int MK>
@@ -172,31 +202,41 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         case PAT_PULL: return &launch_set_eq<S, R, Q, MK, PAT_PULL>;
         case PAT_AA_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_AA_EVEN>;
         case PAT_AA_ODD: return &launch_set_eq<S, R, Q, MK, PAT_AA_ODD>;
-        case PAT_ESO_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_ESO_EVEN>;
-        case PAT_ESO_ODD: return &launch_set_eq<S, R, Q, MK, PAT_ESO_ODD>;
     }
-    if constexpr (sizeof(S) >= 4) {
+    if constexpr (std::is_same<S, e3m12>::value) {
+        return nullptr;   // e3m12: pull and AA
+    } else {
         switch (pat) {
-            case PAT_PUSH: return &launch_set_eq<S, R, Q, MK, PAT_PUSH>;
-            case PAT_EPULL_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_EPULL_EVEN>;
-            case PAT_EPULL_ODD: return &launch_set_eq<S, R, Q, MK, PAT_EPULL_ODD>;
-            case PAT_EPUSH_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_EPUSH_EVEN>;
-            case PAT_EPUSH_ODD: return &launch_set_eq<S, R, Q, MK, PAT_EPUSH_ODD>;
+            case PAT_ESO_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_ESO_EVEN>;
+            case PAT_ESO_ODD: return &launch_set_eq<S, R, Q, MK, PAT_ESO_ODD>;
         }
+        if constexpr (sizeof(S) >= 4) {
+            switch (pat) {
+                case PAT_PUSH: return &launch_set_eq<S, R, Q, MK, PAT_PUSH>;
+                case PAT_EPULL_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_EPULL_EVEN>;
+                case PAT_EPULL_ODD: return &launch_set_eq<S, R, Q, MK, PAT_EPULL_ODD>;
+                case PAT_EPUSH_EVEN: return &launch_set_eq<S, R, Q, MK, PAT_EPUSH_EVEN>;
+                case PAT_EPUSH_ODD: return &launch_set_eq<S, R, Q, MK, PAT_EPUSH_ODD>;
+            }
+        }
+        return nullptr;
     }
-    return nullptr;
 }
 
 // Instantiates the sweep and setter families of one (Q, method) pair in one translation unit.
 // The setter always evaluates the equilibrium in FP64 from FP64 density / velocity fields, so
 // that the density deviation rho - 1 keeps its digits before the PDFs are rounded to storage.
-#define LBM_DEFINE_FAMILY(NAME, Q, MK)                                                          \
+// The families are instantiated in two translation units each (part A: the one-cell sweep, the
+// batched sweep, the boundary pre-pass, the sparse sweeps and the setter; part B: the pair, quad
+// and staged sweeps), so that the build compiles them in parallel.
+#define LBM_DEFINE_FAMILY_A(NAME, Q, MK)                                                          \
     SweepLauncher sweep_##NAME(int store, int pat) {                                            \
         switch (store) {                                                                        \
             case ST_F64: return pick_sweep_pattern<double, double, Q, MK>(pat);                  \
             case ST_F32: return pick_sweep_pattern<float, float, Q, MK>(pat);                    \
             case ST_F16: return pick_sweep_pattern<__half, float, Q, MK>(pat);                   \
             case ST_BF16: return pick_sweep_pattern<__nv_bfloat16, float, Q, MK>(pat);          \
+            case ST_E3M12: return pick_sweep_pattern<e3m12, float, Q, MK>(pat);                 \
         }                                                                                       \
         return nullptr;                                                                         \
     }                                                                                           \
@@ -205,10 +245,43 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         if (store == ST_F32) return pick_batched_pattern<float, float, Q, MK>(pat);             \
         return nullptr;                                                                         \
     }                                                                                           \
+    SweepLauncher prepass_##NAME(int store, int pat) {                                    \
+        switch (store) {                                                                        \
+            case ST_F64: return pick_prepass_pattern<double, double, Q, MK>(pat);          \
+            case ST_F32: return pick_prepass_pattern<float, float, Q, MK>(pat);            \
+            case ST_F16: return pick_prepass_pattern<__half, float, Q, MK>(pat);           \
+            case ST_BF16: return pick_prepass_pattern<__nv_bfloat16, float, Q, MK>(pat);  \
+            case ST_E3M12: return pick_prepass_pattern<e3m12, float, Q, MK>(pat);         \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    SparseLauncher sparse_##NAME(int store) {                                                   \
+        if (store == ST_F64) return &launch_sparse<double, double, Q, MK>;                      \
+        if (store == ST_F32) return &launch_sparse<float, float, Q, MK>;                        \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    SparseSetLauncher sparse_set_##NAME(int store) {                                            \
+        if (store == ST_F64) return &launch_sparse_set<double, double, Q, MK>;                  \
+        if (store == ST_F32) return &launch_sparse_set<float, double, Q, MK>;                   \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    MacroLauncher set_eq_##NAME(int store, int pat) {                                           \
+        switch (store) {                                                                        \
+            case ST_F64: return pick_set_eq_pattern<double, double, Q, MK>(pat);                 \
+            case ST_F32: return pick_set_eq_pattern<float, double, Q, MK>(pat);                   \
+            case ST_F16: return pick_set_eq_pattern<__half, double, Q, MK>(pat);                  \
+            case ST_BF16: return pick_set_eq_pattern<__nv_bfloat16, double, Q, MK>(pat);         \
+            case ST_E3M12: return pick_set_eq_pattern<e3m12, double, Q, MK>(pat);                \
+        }                                                                                       \
+        return nullptr;                                                                         \
+    }
+
+#define LBM_DEFINE_FAMILY_B(NAME, Q, MK)                                                          \
     SweepLauncher sweep_quad_##NAME(int store, int pat) {                                       \
         switch (store) {                                                                        \
             case ST_F16: return pick_quad_pattern<__half, Q, MK>(pat);                           \
             case ST_BF16: return pick_quad_pattern<__nv_bfloat16, Q, MK>(pat);                  \
+            case ST_E3M12: return pick_quad_pattern<e3m12, Q, MK>(pat);                         \
         }                                                                                       \
         return nullptr;                                                                         \
     }                                                                                           \
@@ -221,29 +294,12 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         }                                                                                       \
         return nullptr;                                                                         \
     }                                                                                           \
-    SweepLauncher fixed_density_##NAME(int store, int pat) {                                    \
-        switch (store) {                                                                        \
-            case ST_F64: return pick_fixed_density_pattern<double, double, Q, MK>(pat);          \
-            case ST_F32: return pick_fixed_density_pattern<float, float, Q, MK>(pat);            \
-            case ST_F16: return pick_fixed_density_pattern<__half, float, Q, MK>(pat);           \
-            case ST_BF16: return pick_fixed_density_pattern<__nv_bfloat16, float, Q, MK>(pat);  \
-        }                                                                                       \
-        return nullptr;                                                                         \
-    }                                                                                           \
     SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
         switch (store) {                                                                        \
             case ST_F32: return pick_pair_pattern<float, Q, MK>(pat);                            \
             case ST_F16: return pick_pair_pattern<__half, Q, MK>(pat);                           \
             case ST_BF16: return pick_pair_pattern<__nv_bfloat16, Q, MK>(pat);                  \
-        }                                                                                       \
-        return nullptr;                                                                         \
-    }                                                                                           \
-    MacroLauncher set_eq_##NAME(int store, int pat) {                                           \
-        switch (store) {                                                                        \
-            case ST_F64: return pick_set_eq_pattern<double, double, Q, MK>(pat);                 \
-            case ST_F32: return pick_set_eq_pattern<float, double, Q, MK>(pat);                   \
-            case ST_F16: return pick_set_eq_pattern<__half, double, Q, MK>(pat);                  \
-            case ST_BF16: return pick_set_eq_pattern<__nv_bfloat16, double, Q, MK>(pat);         \
+            case ST_E3M12: return pick_pair_pattern<e3m12, Q, MK>(pat);                         \
         }                                                                                       \
         return nullptr;                                                                         \
     }
@@ -274,10 +330,10 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         return nullptr;                                                                         \
     }                                                                                           \
     SweepLauncher sweep_quad_##NAME(int, int) { return nullptr; }                               \
-    SweepLauncher fixed_density_##NAME(int store, int pat) {                                    \
+    SweepLauncher prepass_##NAME(int store, int pat) {                                    \
         if (pat != PAT_PULL && pat != PAT_AA_EVEN && pat != PAT_AA_ODD) return nullptr;          \
-        if (store == ST_F64) return pick_fixed_density_pattern<double, double, Q, MK>(pat);     \
-        if (store == ST_F32) return pick_fixed_density_pattern<float, float, Q, MK>(pat);       \
+        if (store == ST_F64) return pick_prepass_pattern<double, double, Q, MK>(pat);     \
+        if (store == ST_F32) return pick_prepass_pattern<float, float, Q, MK>(pat);       \
         return nullptr;                                                                         \
     }                                                                                           \
     StagedLauncher sweep_staged_##NAME(int store, int pat) {                                    \
@@ -294,6 +350,16 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         if (store == ST_F32) return NAME##_sweep_pat<float, float>(pat);                        \
         return nullptr;                                                                         \
     }                                                                                           \
+    SparseLauncher sparse_##NAME(int store) {                                                   \
+        if (store == ST_F64) return &launch_sparse<double, double, Q, MK>;                      \
+        if (store == ST_F32) return &launch_sparse<float, float, Q, MK>;                        \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    SparseSetLauncher sparse_set_##NAME(int store) {                                            \
+        if (store == ST_F64) return &launch_sparse_set<double, double, Q, MK>;                  \
+        if (store == ST_F32) return &launch_sparse_set<float, double, Q, MK>;                   \
+        return nullptr;                                                                         \
+    }                                                                                           \
     MacroLauncher set_eq_##NAME(int store, int pat) {                                           \
         if (store == ST_F64) return NAME##_set_pat<double, double>(pat);                        \
         if (store == ST_F32) return NAME##_set_pat<float, double>(pat);                          \
@@ -301,12 +367,14 @@ MacroLauncher pick_set_eq_pattern(int pat) {
     }
 
 #define LBM_DECLARE_FAMILY(NAME)                        \
+    SparseLauncher sparse_##NAME(int store);             \
+    SparseSetLauncher sparse_set_##NAME(int store);      \
     BatchLauncher batched_##NAME(int store, int pat);    \
     SweepLauncher sweep_##NAME(int store, int pat);      \
     SweepLauncher sweep_pair_##NAME(int store, int pat); \
     SweepLauncher sweep_quad_##NAME(int store, int pat); \
     StagedLauncher sweep_staged_##NAME(int store, int pat); \
-    SweepLauncher fixed_density_##NAME(int store, int pat); \
+    SweepLauncher prepass_##NAME(int store, int pat); \
     MacroLauncher set_eq_##NAME(int store, int pat);
 
 LBM_DECLARE_FAMILY(q19_pop)
@@ -315,6 +383,7 @@ LBM_DECLARE_FAMILY(q27_pop)
 LBM_DECLARE_FAMILY(q27_mrt)
 LBM_DECLARE_FAMILY(q27_cum)
 LBM_DECLARE_FAMILY(q27_cum1)
+LBM_DECLARE_FAMILY(q27_cm)
 
 // error reporting shared by the entry points of every translation unit (lbm_abi.cu)
 int abi_fail(int code, const char* fmt, ...);

@@ -80,6 +80,7 @@ __device__ __forceinline__ R collide(R (&f)[Q], const Physics& p) {
     else if constexpr (MK == MK_MRT) return collide_mrt<Q, R>(f, p);
     else if constexpr (MK == MK_CUM1) return collide_cum_ho1<R>(f, p);
     else if constexpr (MK == MK_CUM1_MLP) return collide_cum_ho1<R, true>(f, p, ClosureNu<R>{});
+    else if constexpr (MK == MK_CM) return collide_cm<R>(f, p);
     else return collide_cum<R>(f, p);
 }
 
@@ -116,21 +117,14 @@ __device__ __forceinline__ R load_f_out(const SweepArgs& a, int x, int y, int z,
 }
 
 // Fused boundary handling for a fluid cell next to a boundary: replaces the pulled value of every
-// direction i whose source cell x - c_i is a boundary cell by the value lbmpy's boundary kernel
+// direction i whose source cell x - c_i is a NoSlip or UBB cell by the value lbmpy's boundary kernel
 // would have written there (boundaries/boundaryconditions.py), from the populations the previous
 // step wrote.  f_out(x, j) below is where the previous step wrote direction j of cell x.
-//   NoSlip (:104-139)         f_out(x, inv i)
-//   UBB (:724-841)            f_out(x, inv i) + 6 w_i rho c_i.u_w   (u_w per UBB number or per link)
-//   FreeSlip (:360-455), SimpleExtrapolationOutflow (:844-889)
-//                             f_out(x + off, d)                      (off, d from the link code)
-//   ExtrapolationOutflow (:894-1041)
-//                             c p + (1 - c) p_nd, c = sqrt(1/3); then p <- f_out(x + off, d), p_nd <- result
-//   NoSlipLinearBouzidi (:142-212), wall distance q of the link
-//                             q >= 1/2: (f_out(x, inv i) + (2q - 1) f_out(x, i)) / (2q)
-//                             0 < q < 1/2: 2q f_out(x, inv i) + (1 - 2q) f_out(x + c_i, inv i)
-//                             else f_out(x, inv i)
-// A link whose data table is missing, or whose other cell lies beyond the ghost layer, falls back
-// to NoSlip.
+//   NoSlip (:104-139)   f_out(x, inv i)
+//   UBB (:724-841)      f_out(x, inv i) + 6 w_i rho c_i.u_w   (u_w per UBB number or per link)
+// Links into FixedDensity, FreeSlip, outflow and Bouzidi cells read values of other cells; inside an
+// in-place sweep those cells update concurrently, so k_boundary_prepass stores those links' values
+// where the sweep reads them before the sweep runs, as lbmpy's boundary kernel does.
 template <class S, class R, int Q, int PAT>
 __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const NbrOffsets& nb, int cell,
                                          int x, int y, int z) {
@@ -150,7 +144,11 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
 #pragma unroll
     for (int i = 1; i < Q; ++i) {
         const int bt = g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK;
-        if (bt == 0 || flag_is_fixed_density(bt)) continue;   // FixedDensity: written by k_fixed_density
+        if (bt == 0) continue;
+        // FixedDensity and per-link types: written by k_boundary_prepass (per-link types bounce back
+        // as NoSlip when the plan holds no link tables, so the pre-pass does not run)
+        if (bt >= FLAG_FIXED_DENSITY && !(bt >= FLAG_FREE_SLIP && a.link_code == nullptr && a.link_value == nullptr))
+            continue;
         // f_out(x, inv i): where the previous step wrote direction inv(i) of this cell
         const int j = L::inv(i);
         const int off = nb.off(PA::template woff<Q>(j, 0), PA::template woff<Q>(j, 1), PA::template woff<Q>(j, 2));
@@ -173,31 +171,6 @@ __device__ __forceinline__ void bounce_back(R (&f)[Q], const SweepArgs& a, const
             }
             const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
             v += R(6) * R(L::w(i)) * cu * rho;
-        } else if (bt >= FLAG_FREE_SLIP && bt <= FLAG_OUTFLOW && a.ubb_block != nullptr && a.link_code != nullptr) {
-            const size_t li = size_t(a.ubb_block[icell]) * Q + size_t(j);
-            const int code = a.link_code[li];
-            const R w = load_f_out<S, R, Q, PAT>(a, x, y, z, link_off(code, 0), link_off(code, 1), link_off(code, 2),
-                                                 link_dir(code), v);
-            if (bt == FLAG_OUTFLOW && a.link_value != nullptr) {
-                double* st = a.link_value + li * 2;
-                const R c = R(0.57735026918962576451);   // sqrt(1/3) dt/dx
-                const R fin = c * R(st[0]) + (R(1) - c) * R(st[1]);
-                st[0] = double(w);
-                st[1] = double(fin);
-                v = fin;
-            } else {
-                v = w;
-            }
-        } else if (bt == FLAG_BOUZIDI && a.ubb_block != nullptr && a.link_value != nullptr) {
-            const R q = R(a.link_value[(size_t(a.ubb_block[icell]) * Q + size_t(j)) * 2]);
-            if (q >= R(0.5)) {
-                const int oi = nb.off(PA::template woff<Q>(i, 0), PA::template woff<Q>(i, 1), PA::template woff<Q>(i, 2));
-                const R finv = Conv<S, R>::ld(src + eidx(PA::template wslot<Q>(i) * g.sq, cell + oi));
-                v = (R(0.5) * (v + finv * (R(2) * q - R(1)))) / q;
-            } else if (q > R(0)) {
-                const R d2 = load_f_out<S, R, Q, PAT>(a, x, y, z, L::cx(i), L::cy(i), L::cz(i), j, v);
-                v = R(2) * q * v + (R(1) - R(2) * q) * d2;
-            }
         }
         f[i] = v;
     }
@@ -239,8 +212,19 @@ __device__ __forceinline__ void sweep_cell(const SweepArgs& a, int x, int y, int
     if (a.omega_out != nullptr) a.omega_out[x + g.nx * (y + (long long)g.ny * z)] = (float)om;
 }
 
+// Resident 256-thread blocks per SM that the one-cell sweep is compiled for.  The register
+// allocator otherwise trades occupancy for registers in ways that move with unrelated code (the
+// near-wall path): the D3Q27 cumulant AA odd sweep went from 80 to 92 registers (3 to 2 blocks)
+// when the per-link boundary data arrived.  These hot variants are held to the register counts
+// at which they ran at HBM speed (-Xptxas -v): 80 (3 blocks), 64 (4) and 48 (5).
+template <class S, int Q, int MK, int PAT> struct SweepMinBlocks { static constexpr int value = 1; };
+template <> struct SweepMinBlocks<float, 27, MK_CUM1, PAT_AA_ODD> { static constexpr int value = 3; };
+template <> struct SweepMinBlocks<float, 27, MK_CUM1, PAT_AA_EVEN> { static constexpr int value = 4; };
+template <> struct SweepMinBlocks<float, 19, MK_POP, PAT_PULL> { static constexpr int value = 5; };
+template <> struct SweepMinBlocks<float, 19, MK_MRT, PAT_PULL> { static constexpr int value = 3; };
+
 template <class S, class R, int Q, int MK, int PAT>
-__global__ void __launch_bounds__(256) k_sweep(const SweepArgs a) {
+__global__ void __launch_bounds__(256, SweepMinBlocks<S, Q, MK, PAT>::value) k_sweep(const SweepArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
@@ -356,6 +340,104 @@ __global__ void __launch_bounds__(256, 2) k_sweep_batched(const BatchArgs b) {
     }
 }
 
+// ------------------------------------------------------------------ sparse (list-based) domains
+// lbmpy's sparse LBM (sparse/mapping.py:13-156, sparse/update_rule_sparse.py:22-52): the cells are a
+// list (fluid cells first, then boundary cells), PDF i of list cell c at element c + i * n_cells, and
+// an index list gives, per fluid cell and direction i >= 1, the element a pull sweep reads
+// (a neighbour's slot, the cell's own inverse slot for NoSlip, or the periodic image).  Index
+// layout here: [Q-1][n_fluid] (direction-major, so a warp's reads of one direction are coalesced).
+struct SparseArgs {
+    Physics p;
+    const void* src;
+    void* dst;
+    const unsigned* index;
+    long long n_fluid;
+    long long n_cells;
+};
+
+template <class S, class R, int Q, int MK>
+__global__ void __launch_bounds__(256) k_sweep_sparse(const SparseArgs a) {
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= a.n_fluid) return;
+    const S* src = static_cast<const S*>(a.src);
+    S* dst = static_cast<S*>(a.dst);
+    R f[Q];
+    f[0] = Conv<S, R>::ld(src + c);
+#pragma unroll
+    for (int i = 1; i < Q; ++i) f[i] = Conv<S, R>::ld(src + a.index[(long long)(i - 1) * a.n_fluid + c]);
+    collide<R, Q, MK>(f, a.p);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) Conv<S, R>::st(dst + c + (long long)i * a.n_cells, f[i]);
+}
+
+// Equilibrium of list cells c < n_fluid from rho[c] and u[k * n_fluid + c] (FP64).  The velocity
+// enters unshifted, as lbmpy's sparse setter builds it (force_substitution=False,
+// sparse/update_rule_sparse.py:70-85).
+template <class S, class R, int Q, int MK>
+__global__ void __launch_bounds__(256) k_sparse_set_equilibrium(const SparseArgs a, const double* rho,
+                                                               const double* u) {
+    constexpr int EQ = (MK == MK_CUM1 || MK == MK_CUM1_MLP) ? MK_CUM : MK;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= a.n_fluid) return;
+    const R r = R(rho[c]);
+    const R ux = R(u[c]), uy = R(u[a.n_fluid + c]), uz = R(u[2 * a.n_fluid + c]);
+    R f[Q];
+    equilibrium<Q, R, EQ>(f, r, ux, uy, uz, a.p);
+    S* dst = static_cast<S*>(a.dst);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) Conv<S, R>::st(dst + c + (long long)i * a.n_cells, f[i]);
+}
+
+// Velocity bounce-back on a sparse list (lbmpy's SparseLbBoundaryMapper with UBB,
+// sparse/mapping.py:157-247 and boundaries/boundaryconditions.py UBB): link k runs from fluid cell
+// links[n_links + k] in direction links[k] into boundary cell links[2 * n_links + k]; the boundary
+// cell's slot inv(d), which the fluid cell pulls next, receives f_out(c, d) - 6 w_d rho (c_d . u_w)
+// (rho the cell's density when compressible, else 1).  Runs on the source list before the sweep;
+// each link writes its own slot, and only boundary cells are written.
+template <class S, class R, int Q>
+__global__ void __launch_bounds__(256) k_sparse_ubb(const SparseArgs a, const unsigned* links, long long n_links,
+                                                    double ux, double uy, double uz) {
+    using L = Lat<Q>;
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= n_links) return;
+    const int d = int(links[k]);
+    if (d < 1 || d >= Q) return;
+    const long long c = links[n_links + k], b = links[2 * n_links + k];
+    S* pdf = static_cast<S*>(a.dst);
+    R rho = R(1);
+    if (a.p.compressible) {
+        R s = R(0);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) s += Conv<S, R>::ld(pdf + c + (long long)i * a.n_cells);
+        rho += s;
+    }
+    const R cu = R(L::cx(d)) * R(ux) + R(L::cy(d)) * R(uy) + R(L::cz(d)) * R(uz);
+    const R v = Conv<S, R>::ld(pdf + c + (long long)d * a.n_cells) - R(6) * R(L::w(d)) * cu * rho;
+    Conv<S, R>::st(pdf + b + (long long)L::inv(d) * a.n_cells, v);
+}
+
+// Density and velocity (FP64) of list cells c < n_fluid (sparse/update_rule_sparse.py:55-67).
+template <class S, class R, int Q>
+__global__ void __launch_bounds__(256) k_sparse_get_macroscopic(const SparseArgs a, double* rho, double* u) {
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= a.n_fluid) return;
+    const S* src = static_cast<const S*>(a.src);
+    R f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = Conv<S, R>::ld(src + c + (long long)i * a.n_cells);
+    Macro<Q, R> m = conserved<Q, R>(f, a.p, false);
+    if (a.p.force_model != FM_NONE) {
+        const R h = R(0.5) / m.rho_ref;
+        m.ux += h * R(a.p.force[0]); m.uy += h * R(a.p.force[1]); m.uz += h * R(a.p.force[2]);
+    }
+    if (rho) rho[c] = m.rho;
+    if (u) {
+        u[c] = m.ux;
+        u[a.n_fluid + c] = m.uy;
+        u[2 * a.n_fluid + c] = m.uz;
+    }
+}
+
 // ------------------------------------------------------------------ setter / getter
 struct MacroArgs {
     Grid g;
@@ -400,16 +482,26 @@ __global__ void __launch_bounds__(256) k_set_equilibrium(const MacroArgs a) {
     }
 }
 
-// FixedDensity links (boundaries/boundaryconditions.py:1044-1099), before the sweep as lbmpy's
-// boundary kernel runs before its sweep.  For a fluid cell x whose neighbour x - c_i is a
-// FixedDensity cell, the population the sweep reads in direction i becomes
-//   2 feq_even_i(rho_w, u) - f*_{inv i}(x),   feq_even_i = (feq_i + feq_{inv i}) / 2,
-// the part of the method's equilibrium that is even in u, with u from x's outgoing populations of
-// the previous step at density rho_w (j / rho_w compressible, j otherwise).  It is stored where
-// the sweep reads it: a slot that only the boundary cell's own update would write, so no fluid
-// cell's outgoing value is overwritten, in place or not.  Force-free methods (host-checked).
+// Boundary pre-pass, before the sweep as lbmpy's boundary kernel runs before its sweep: for every
+// fluid cell x next to a cell of a type whose incoming value depends on other cells' populations,
+// compute that value per link and store it where the sweep reads direction i of x (a slot that only
+// the boundary cell's own update would write, so no fluid cell's outgoing value is overwritten, in
+// place or not).  f_out(y, d) is where the previous step wrote direction d of cell y; the link from
+// x towards the boundary cell x - c_i has direction j = inv(i).
+//   FixedDensity (:1044-1099)            2 feq_even_i(rho_w, u) - f_out(x, j),  feq_even_i =
+//                                        (feq_i + feq_j) / 2, u from x's outgoing populations at
+//                                        density rho_w (j / rho_w compressible, j otherwise);
+//                                        force-free methods (host-checked)
+//   FreeSlip (:360-455), SimpleExtrapolationOutflow (:844-889)
+//                                        f_out(x + off, d)          (off, d from the link code)
+//   ExtrapolationOutflow (:894-1041)     c p + (1 - c) p_nd, c = sqrt(1/3); then
+//                                        p <- f_out(x + off, d), p_nd <- the result
+//   NoSlipLinearBouzidi (:142-212)       q >= 1/2: (f_out(x, j) + (2q - 1) f_out(x, i)) / (2q)
+//                                        0 < q < 1/2: 2q f_out(x, j) + (1 - 2q) f_out(x + c_i, j)
+//                                        else f_out(x, j)
+// A link whose table is missing, or whose other cell lies beyond the ghost layer, gets NoSlip.
 template <class S, class R, int Q, int MK, int PAT>
-__global__ void __launch_bounds__(256) k_fixed_density(const SweepArgs a) {
+__global__ void __launch_bounds__(256) k_boundary_prepass(const SweepArgs a) {
     using L = Lat<Q>;
     using A = Access<PAT>;
     using PA = Access<PrevPattern<PAT>::value>;
@@ -429,42 +521,87 @@ __global__ void __launch_bounds__(256) k_fixed_density(const SweepArgs a) {
         gf.sz = g.fsz;
         fo.init(gf, x, y, z);
     }
-    unsigned types = 0;   // bit 0: a link to a type-6 cell, bit 1: to a type-7 cell
+    unsigned types = 0;   // bit t: a link to a cell of type t
 #pragma unroll
-    for (int i = 1; i < Q; ++i) {
-        const int t = g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK;
-        if (flag_is_fixed_density(t)) types |= 1u << (t - FLAG_FIXED_DENSITY);
-    }
-    if (!types) return;
+    for (int i = 1; i < Q; ++i)
+        types |= 1u << (g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK);
+    constexpr unsigned HANDLED = (1u << FLAG_FIXED_DENSITY) | (1u << FLAG_FIXED_DENSITY1) | (1u << FLAG_FREE_SLIP) |
+                                 (1u << FLAG_SIMPLE_OUTFLOW) | (1u << FLAG_OUTFLOW) | (1u << FLAG_BOUZIDI);
+    if (!(types & HANDLED)) return;
     NbrOffsets nb;
     nb.init(g, x, y, z);
     const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
     S* f = const_cast<S*>(static_cast<const S*>(a.src));
     R out[Q];
-    R jx = 0, jy = 0, jz = 0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const int off = nb.off(PA::template woff<Q>(k, 0), PA::template woff<Q>(k, 1), PA::template woff<Q>(k, 2));
         out[k] = Conv<S, R>::ld(f + eidx(PA::template wslot<Q>(k) * g.sq, cell + off));
-        jx += R(L::cx(k)) * out[k];
-        jy += R(L::cy(k)) * out[k];
-        jz += R(L::cz(k)) * out[k];
     }
-#pragma unroll 1
-    for (int t = 0; t < 2; ++t) {
-        if (!((types >> t) & 1u)) continue;
-        const R rw = R(t == 0 ? a.p.fixed_density : a.p.fixed_density1);
-        const R s = a.p.compressible ? R(1) / rw : R(1);
-        R feq[Q];
-        equilibrium<Q, R, EQ>(feq, rw, jx * s, jy * s, jz * s, a.p);
+    // where the sweep reads direction i of this cell
+    auto store = [&](int i, R v) {
+        const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
+        Conv<S, R>::st(f + eidx(A::template rslot<Q>(i) * g.sq, cell + off), v);
+    };
+    if (types & ((1u << FLAG_FIXED_DENSITY) | (1u << FLAG_FIXED_DENSITY1))) {
+        R jx = 0, jy = 0, jz = 0;
 #pragma unroll
-        for (int i = 1; i < Q; ++i) {
-            if ((g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK) != FLAG_FIXED_DENSITY + t)
-                continue;
-            const int q = L::inv(i);
-            const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
-            Conv<S, R>::st(f + eidx(A::template rslot<Q>(i) * g.sq, cell + off), feq[q] + feq[i] - out[q]);
+        for (int k = 0; k < Q; ++k) {
+            jx += R(L::cx(k)) * out[k];
+            jy += R(L::cy(k)) * out[k];
+            jz += R(L::cz(k)) * out[k];
         }
+#pragma unroll 1
+        for (int t = 0; t < 2; ++t) {
+            if (!((types >> (FLAG_FIXED_DENSITY + t)) & 1u)) continue;
+            const R rw = R(t == 0 ? a.p.fixed_density : a.p.fixed_density1);
+            const R s = a.p.compressible ? R(1) / rw : R(1);
+            R feq[Q];
+            equilibrium<Q, R, EQ>(feq, rw, jx * s, jy * s, jz * s, a.p);
+#pragma unroll
+            for (int i = 1; i < Q; ++i) {
+                if ((g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK) != FLAG_FIXED_DENSITY + t)
+                    continue;
+                const int q = L::inv(i);
+                store(i, feq[q] + feq[i] - out[q]);
+            }
+        }
+    }
+    if (!(types & ((1u << FLAG_FREE_SLIP) | (1u << FLAG_SIMPLE_OUTFLOW) | (1u << FLAG_OUTFLOW) | (1u << FLAG_BOUZIDI))))
+        return;
+    const int icell = x + g.nx * (y + g.ny * z);
+    const int blk = a.ubb_block != nullptr ? a.ubb_block[icell] : -1;
+#pragma unroll
+    for (int i = 1; i < Q; ++i) {
+        const int bt = g.flags[fcell + fo.off(-L::cx(i), -L::cy(i), -L::cz(i))] & FLAG_TYPE_MASK;
+        if (bt < FLAG_FREE_SLIP || bt > FLAG_BOUZIDI) continue;
+        const int j = L::inv(i);
+        R v = out[j];                                  // NoSlip fallback
+        if (blk >= 0 && bt <= FLAG_OUTFLOW && a.link_code != nullptr) {
+            const size_t li = size_t(blk) * Q + size_t(j);
+            const int code = a.link_code[li];
+            const R w = load_f_out<S, R, Q, PAT>(a, x, y, z, link_off(code, 0), link_off(code, 1), link_off(code, 2),
+                                                 link_dir(code), v);
+            if (bt == FLAG_OUTFLOW && a.link_value != nullptr) {
+                double* st = a.link_value + li * 2;
+                const R c = R(0.57735026918962576451);   // sqrt(1/3) dt/dx
+                const R fin = c * R(st[0]) + (R(1) - c) * R(st[1]);
+                st[0] = double(w);
+                st[1] = double(fin);
+                v = fin;
+            } else {
+                v = w;
+            }
+        } else if (blk >= 0 && bt == FLAG_BOUZIDI && a.link_value != nullptr) {
+            const R q = R(a.link_value[(size_t(blk) * Q + size_t(j)) * 2]);
+            if (q >= R(0.5)) {
+                v = (R(0.5) * (out[j] + out[i] * (R(2) * q - R(1)))) / q;
+            } else if (q > R(0)) {
+                const R d2 = load_f_out<S, R, Q, PAT>(a, x, y, z, L::cx(i), L::cy(i), L::cz(i), j, out[j]);
+                v = R(2) * q * out[j] + (R(1) - R(2) * q) * d2;
+            }
+        }
+        store(i, v);
     }
 }
 

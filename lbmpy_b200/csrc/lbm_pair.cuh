@@ -48,6 +48,7 @@ __device__ __forceinline__ F2& operator-=(F2& a, F2Prod b) { a = a - b; return a
 __device__ __forceinline__ F2& operator*=(F2& a, F2 b) { a = F2(__fmul2_rn(a.v, b.v)); return a; }
 __device__ __forceinline__ F2 operator/(F2 a, F2 b) { return F2(a.v.x / b.v.x, a.v.y / b.v.y); }
 __device__ __forceinline__ F2 sqrt(F2 a) { return F2(sqrtf(a.v.x), sqrtf(a.v.y)); }
+__device__ __forceinline__ F2 fabs(F2 a) { return F2(fabsf(a.v.x), fabsf(a.v.y)); }
 
 // ------------------------------------------------------------------ paired storage access
 template <class S> struct Pair;
@@ -92,9 +93,18 @@ constexpr int PAIR_ROWS = 4;
 // the sweep is limited by latency rather than bandwidth at the occupancy its registers allow; a
 // cap of 80 registers (6 blocks) trades a few spilled words for a third more resident warps.
 // FP32: 5 blocks (at most 102 registers); without a stated minimum the allocator may take far more.
+template <> struct Pair<e3m12> {
+    using V = unsigned;
+    __device__ __forceinline__ static V ld(const e3m12* p) { return *reinterpret_cast<const unsigned*>(p); }
+    __device__ __forceinline__ static void st(e3m12* p, V v) { *reinterpret_cast<unsigned*>(p) = v; }
+    __device__ __forceinline__ static float2 to_f2(V v) { return make_float2(e3m12_decode(v & 0xffffu), e3m12_decode(v >> 16)); }
+    __device__ __forceinline__ static V from_f2(float2 v) { return e3m12_encode(v.x) | (e3m12_encode(v.y) << 16); }
+};
+
 template <class S> struct PairMinBlocks { static constexpr int value = 5; };
 template <> struct PairMinBlocks<__half> { static constexpr int value = 6; };
 template <> struct PairMinBlocks<__nv_bfloat16> { static constexpr int value = 6; };
+template <> struct PairMinBlocks<e3m12> { static constexpr int value = 6; };
 
 template <class S, int Q, int MK, int PAT>
 __global__ void __launch_bounds__(32 * PAIR_ROWS, PairMinBlocks<S>::value) k_sweep_pair(const SweepArgs a) {

@@ -1,0 +1,6 @@
+// Kernel instantiations: D3Q27 central-moment collision, FP64 / FP32 storage, pull and AA.
+#include "lbm_dispatch.h"
+
+namespace lbm {
+LBM_DEFINE_FAMILY_REDUCED(q27_cm, 27, MK_CM)
+}  // namespace lbm

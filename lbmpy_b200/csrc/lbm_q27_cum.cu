@@ -1,6 +1,7 @@
-// Kernel instantiations: D3Q27, CUM collision, every storage type and pattern.
+// Kernel instantiations, part A: D3Q27, cumulant collision with general rates, every storage type
+// and pattern; the one-cell, batched and sparse sweeps, the boundary pre-pass and the setter.
 #include "lbm_dispatch.h"
 
 namespace lbm {
-LBM_DEFINE_FAMILY(q27_cum, 27, MK_CUM)
+LBM_DEFINE_FAMILY_A(q27_cum, 27, MK_CUM)
 }  // namespace lbm

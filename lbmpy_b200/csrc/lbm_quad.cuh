@@ -28,6 +28,15 @@ template <> struct Quad<__nv_bfloat16> {
     }
 };
 
+template <> struct Quad<e3m12> {
+    __device__ __forceinline__ static float2 to_f2(unsigned w) {
+        return make_float2(e3m12_decode(w & 0xffffu), e3m12_decode(w >> 16));
+    }
+    __device__ __forceinline__ static unsigned from_f2(float2 v) {
+        return e3m12_encode(v.x) | (e3m12_encode(v.y) << 16);
+    }
+};
+
 template <class S>
 __device__ __forceinline__ void quad_ld(const S* p, float (&v)[4]) {
     const uint2 w = *reinterpret_cast<const uint2*>(p);

@@ -13,7 +13,8 @@
 // 16-bit storage the aligned 4-byte word holding it, whose other half lies in the row or in its
 // padding).  Each cell's flag is loaded one tile ahead.  Writes go straight to global memory.
 //
-// Every wait on a barrier is bounded (STAGED_WAIT_NS); a CTA whose stage does not complete sets
+// Every wait on a barrier is bounded (SweepArgs::stage_wait_ns, default STAGED_WAIT_NS); a CTA
+// whose stage does not complete sets
 // the plan's device status word, waits for its own copies in flight and returns.
 //
 // Opt-in (LBM_B200_STAGED=1).  Measured on B200 it matches but does not beat the other sweeps
@@ -74,14 +75,14 @@ __device__ __forceinline__ unsigned long long now_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Phase `parity` of the barrier completed; false once STAGED_WAIT_ITERS polls or STAGED_WAIT_NS
+// Phase `parity` of the barrier completed; false once STAGED_WAIT_ITERS polls or `limit_ns`
 // have passed without it.
-__device__ __forceinline__ bool wait(unsigned bar, unsigned parity) {
+__device__ __forceinline__ bool wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
     if (try_wait(bar, parity)) return true;
     const unsigned long long t0 = now_ns();
     for (unsigned it = 1; it < STAGED_WAIT_ITERS; ++it) {
         if (try_wait(bar, parity)) return true;
-        if ((it & 255u) == 0 && now_ns() - t0 > STAGED_WAIT_NS) return false;
+        if ((it & 15u) == 0 && now_ns() - t0 > limit_ns) return false;
     }
     return false;
 }
@@ -123,7 +124,8 @@ __device__ __forceinline__ void staged_warp_dispatch(int warp, F&& f) {
 // element after a row's ghost cell lies in the row's padding); 2 <= ns <= STAGED_MAX_NS.
 //
 // Shared memory: mbarriers (64 B), the tile header of each stage (8 x 16 B), the headers of the
-// next two tiles to issue (2 x 16 B), thread 0's tile iterator, then the stages.
+// next two tiles to issue (2 x 16 B), thread 0's tile iterator (24 B), the probe barrier (8 B at
+// byte 248), then the stages.
 template <class S, class R, int Q, int MK, int PAT, int W>
 __global__ void __launch_bounds__(W) k_sweep_staged(const SweepArgs a, const int ns) {
     static_assert(PAT == PAT_PULL || PAT == PAT_AA_EVEN || PAT == PAT_AA_ODD, "staged sweep: pull and AA");
@@ -150,8 +152,11 @@ __global__ void __launch_bounds__(W) k_sweep_staged(const SweepArgs a, const int
     const S* src = static_cast<const S*>(a.src);
     S* dst = static_cast<S*>(a.dst);
 
+    const unsigned long long wait_ns = a.stage_wait_ns != 0 ? a.stage_wait_ns : STAGED_WAIT_NS;
+    const unsigned probe_bar = bar0 + 248;
     if (tid == 0) {
         for (int s = 0; s < ns; ++s) staged::bar_init(bar0 + 8 * s, W);
+        if (a.stage_probe) staged::bar_init(probe_bar, 1);
         staged::fence_bar_init();
         // CTA b sweeps tiles b, b + G, b + 2G, ... (walls spread over all CTAs); the step G is
         // added to (segment, y, z) with carries
@@ -227,7 +232,10 @@ __global__ void __launch_bounds__(W) k_sweep_staged(const SweepArgs a, const int
 
     for (int k = 0; k < mine; ++k) {
         const int s = k % ns;
-        const bool ok = staged::wait(bar0 + 8 * s, unsigned(k / ns) & 1u);
+        bool ok = staged::wait(bar0 + 8 * s, unsigned(k / ns) & 1u, wait_ns);
+        // probe: the last tile's data have landed and no copy is in flight; a wait on a barrier
+        // that no thread arrives at runs out after wait_ns
+        if (a.stage_probe && k == mine - 1) ok = ok && staged::wait(probe_bar, 0u, wait_ns);
         const S* st = stage0 + s * STAGE_ELEMS;
         const StagedTile t = hdr[s];
         R f[Q];

@@ -10,8 +10,10 @@ from __future__ import annotations
 
 import torch
 
+# e3m12 (1 sign, 3 exponent, 12 mantissa bits, scaled by 16; include/lbm_b200.h) has no torch type:
+# its 16-bit codes live in an int16 tensor
 _TORCH_DTYPES = {"float64": torch.float64, "float32": torch.float32, "float16": torch.float16,
-                 "bfloat16": torch.bfloat16}
+                 "bfloat16": torch.bfloat16, "e3m12": torch.int16}
 ALIGN_BYTES = 32
 
 

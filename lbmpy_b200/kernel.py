@@ -20,10 +20,12 @@ from .enums import Timestep, is_inplace
 from .fields import check_pdf_tensor
 from . import forcemodels
 
-_METHOD = {"srt": N.METHOD_SRT, "trt": N.METHOD_TRT, "mrt": N.METHOD_MRT, "cumulant": N.METHOD_CUMULANT}
+_METHOD = {"srt": N.METHOD_SRT, "trt": N.METHOD_TRT, "mrt": N.METHOD_MRT, "cumulant": N.METHOD_CUMULANT,
+           "central_moment": N.METHOD_CENTRAL_MOMENT}
 _PATTERN = {"pull": N.PATTERN_PULL, "aa": N.PATTERN_AA, "esotwist": N.PATTERN_ESOTWIST, "push": N.PATTERN_PUSH,
             "esopull": N.PATTERN_ESOPULL, "esopush": N.PATTERN_ESOPUSH}
-_DT = {"float64": N.DTYPE_F64, "float32": N.DTYPE_F32, "float16": N.DTYPE_F16, "bfloat16": N.DTYPE_BF16}
+_DT = {"float64": N.DTYPE_F64, "float32": N.DTYPE_F32, "float16": N.DTYPE_F16, "bfloat16": N.DTYPE_BF16,
+       "e3m12": N.DTYPE_E3M12}
 
 
 def _evaluate(value, params: Dict, placeholder=None):
@@ -91,6 +93,7 @@ def build_desc(update_rule, dims, periodic, params: Dict, ubb_velocities=None,
         for k in range(3):
             d.force[k] = f[k]
     d.galilean_correction = int(bool(rule.galilean_correction))
+    d.fourth_order_limiter = float(getattr(rule, "fourth_order_limiter", 0.0))
     shear = _evaluate(m.shear_relaxation_rate, params, ph)
     d.shear_rate = shear
     if rule.subgrid_scale_model is not None:

@@ -217,6 +217,23 @@ def cumulant_groups() -> List[List[Poly]]:
     ]
 
 
+def fourth_order_rates(w1, w2):
+    """The third-order rates (w3, w4, w5) before the per-cell limiters, and the parameters (a, b), of
+    the fourth-order cumulant correction for shear rate w1 and bulk rate w2 (Geier et al. 2017,
+    eq. 111-116; methods/cumulantbased/fourth_order_correction.py:79-97, :149-170).  Works on numbers
+    and on sympy expressions."""
+    w11, w12, w22 = w1 * w1, w1 * w2, w2 * w2
+    w3 = 8 * (w1 - 2) * (w2 * (3 * w1 - 1) - 5 * w1) / (8 * (5 - 2 * w1) * w1 + w2 * (8 + w1 * (9 * w1 - 26)))
+    w4 = 8 * (w1 - 2) * (w1 + w2 * (3 * w1 - 7)) / (w2 * (56 - 42 * w1 + 9 * w11) - 8 * w1)
+    w5 = 24 * (w1 - 2) * (4 * w11 + w12 * (18 - 13 * w1) + w22 * (2 + w1 * (6 * w1 - 11))) / (
+        16 * w11 * (w1 - 6) - 2 * w12 * (216 + 5 * w1 * (9 * w1 - 46))
+        + w22 * (w1 * (3 * w1 - 10) * (15 * w1 - 28) - 48))
+    den = (w1 - w2) * (w2 * (2 + 3 * w1) - 8 * w1)
+    a = (4 * w11 + 2 * w12 * (w1 - 6) + w22 * (w1 * (10 - 3 * w1) - 4)) / den
+    b = (4 * w12 * (9 * w1 - 16) - 4 * w11 - 2 * w22 * (2 + 9 * w1 * (w1 - 2))) / (3 * den)
+    return (w3, w4, w5), (a, b)
+
+
 def rates_for_groups(rates: Sequence[float], groups: List[List[Poly]], dim: int,
                      conserved_moments: bool = True) -> List[float]:
     """Per-moment relaxation rates in group order, following lbmpy's rule

@@ -1,8 +1,8 @@
-"""Storage-precision study: the same Taylor-Green run stored in FP64, FP32, FP16 and BF16.
+"""Storage-precision study: the same Taylor-Green run stored in FP64, FP32, FP16, BF16 and e3m12.
 
 The D3Q19 TRT periodic box (relaxation rate 1.8, magic-number odd rate, compressible) starts
 from a Taylor-Green vortex u0 = 0.04 in x/y plus seeded Gaussian noise (sigma 1e-3); every run
-uses the same initial field.  FP16 / BF16 store zero-centred PDFs (f - w_i, lbmpy's
+uses the same initial field.  FP16 / BF16 / e3m12 store zero-centred PDFs (f - w_i, lbmpy's
 zero-centring) and collide in FP32 registers.  Reported per storage type, against the FP64 run:
 the relative L2 velocity error at the end and along the way, and the kinetic-energy history
 (FP64 reduction on the GPU), with GLUPS.
@@ -64,7 +64,7 @@ def _run(n, storage, steps, every, u_init, device):
 
 
 def precision_study(n: int = 512, steps: int = 5000, every: int = 500, seed: int = 0,
-                    storages=("float32", "float16", "bfloat16"), device="cuda", log=print):
+                    storages=("float32", "float16", "bfloat16", "e3m12"), device="cuda", log=print):
     t0 = time.time()
     u0 = tgv_field(n, seed=seed, device=device)
     ref = _run(n, "float64", steps, every, u0, device)

@@ -25,6 +25,9 @@
  * (fzyx = x fastest, PDF index slowest, is the default).  Parity status: see oracle_spec.py.
  */
 #include <math.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -64,6 +67,7 @@ typedef struct {
     const int* link_code;     /* flags 8-10: per-link source, dir | (ox+1)<<8 | (oy+1)<<10 | (oz+1)<<12,
                                  [cell][q] (interior cells, x fastest; q the link direction) */
     double* link_value;       /* flags 10, 11: per-link values [cell][q][2] (outflow state, Bouzidi q) */
+    double foc_limiter;       /* > 0: fourth-order cumulant correction with this limiter */
 } om_method;
 
 typedef struct {
@@ -437,6 +441,97 @@ void om_mlp_features(const double* P6, double rho, const double* u, double* x) {
     mlp_features(P, rho, u, x);
 }
 
+/* Index of the method's polynomial whose monomial row (M[k][.], monomials a*9 + b*3 + c) has exactly
+ * the n given entries, or -1. */
+static int poly_row(const om_method* m, int n, const int* mono, const double* coef) {
+    int k, j, t;
+    for (k = 0; k < m->Q; ++k) {
+        int ok = 1;
+        for (j = 0; j < 27 && ok; ++j) {
+            double want = 0.0;
+            for (t = 0; t < n; ++t) if (mono[t] == j) want = coef[t];
+            if (m->M[k][j] != want) ok = 0;
+        }
+        if (ok) return k;
+    }
+    return -1;
+}
+
+#define MONO(a, b, c) ((a) * 9 + (b) * 3 + (c))
+
+/* Fourth-order correction of the polynomial cumulant collision (Geier et al. 2017, eq. 44-49 and
+ * 112-116; methods/cumulantbased/fourth_order_correction.py:21-237): the third-order groups relax
+ * with limited rates, and the fourth-order polynomials PC1..PC6 receive correction terms built from
+ * the velocity-derivative estimates of the second-order cumulants.  cmono: pre-collision monomial
+ * cumulants (rho-scaled); cpoly / cpost: pre- / post-collision polynomial cumulants. */
+static void fourth_order_correction(const om_method* m, double rho, const double* cmono, const double* cpoly,
+                                    double* cpost) {
+    static const double one = 1.0;
+    const double p11[2] = {1.0, 1.0}, p1m[2] = {1.0, -1.0}, pc1[3] = {1.0, -2.0, 1.0},
+                 pc2[3] = {1.0, 1.0, -2.0}, pc3[3] = {1.0, 1.0, 1.0};
+    /* third-order groups: sums, differences (each of the three permutations), xyz */
+    const int sums[3][2] = {{MONO(1, 2, 0), MONO(1, 0, 2)}, {MONO(2, 1, 0), MONO(0, 1, 2)},
+                            {MONO(2, 0, 1), MONO(0, 2, 1)}};
+    const int m4[3] = {MONO(2, 2, 0), MONO(2, 0, 2), MONO(0, 2, 2)};
+    const int xy = MONO(1, 1, 0), xz = MONO(1, 0, 1), yz = MONO(0, 1, 1), x2 = MONO(2, 0, 0),
+              y2 = MONO(0, 2, 0), z2 = MONO(0, 0, 2), xyz = MONO(1, 1, 1);
+    const int bulk[3] = {x2, y2, z2};
+    int ks[3], kd[3], k5, kp[6], j, kxy, kb;
+    double w1, w2, w3, w4, w5, w6, w7, w8, lim, a, b, den, w11, w12, w22, dx, dy, dz, dxy, dxz, dyz, g, t;
+    for (j = 0; j < 3; ++j) {
+        ks[j] = poly_row(m, 2, sums[j], p11);
+        kd[j] = poly_row(m, 2, sums[j], p1m);
+    }
+    k5 = poly_row(m, 1, &xyz, &one);
+    kp[0] = poly_row(m, 3, m4, pc1);
+    kp[1] = poly_row(m, 3, m4, pc2);
+    kp[2] = poly_row(m, 3, m4, pc3);
+    {
+        const int p4 = MONO(2, 1, 1), p5 = MONO(1, 2, 1), p6 = MONO(1, 1, 2);
+        kp[3] = poly_row(m, 1, &p4, &one);
+        kp[4] = poly_row(m, 1, &p5, &one);
+        kp[5] = poly_row(m, 1, &p6, &one);
+    }
+    kxy = poly_row(m, 1, &xy, &one);
+    kb = poly_row(m, 3, bulk, pc3);
+    w1 = m->rate[kxy];
+    w2 = m->rate[kb];
+    w6 = m->rate[kp[0]]; w7 = m->rate[kp[2]]; w8 = m->rate[kp[3]];
+    /* limited third-order rates (fourth_order_correction.py:199-211) */
+    lim = rho * m->foc_limiter;
+    t = fabs(cmono[MONO(1, 2, 0)] + cmono[MONO(1, 0, 2)]);
+    w3 = m->rate[ks[0]] + (1.0 - m->rate[ks[0]]) * t / (lim + t);
+    t = fabs(cmono[MONO(1, 2, 0)] - cmono[MONO(1, 0, 2)]);
+    w4 = m->rate[kd[0]] + (1.0 - m->rate[kd[0]]) * t / (lim + t);
+    t = fabs(cmono[xyz]);
+    w5 = m->rate[k5] + (1.0 - m->rate[k5]) * t / (lim + t);
+    for (j = 0; j < 3; ++j) {          /* third-order equilibria are zero */
+        cpost[ks[j]] = cpoly[ks[j]] - w3 * cpoly[ks[j]];
+        cpost[kd[j]] = cpoly[kd[j]] - w4 * cpoly[kd[j]];
+    }
+    cpost[k5] = cpoly[k5] - w5 * cpoly[k5];
+    /* a and b (eq. 115-116) */
+    w11 = w1 * w1; w12 = w1 * w2; w22 = w2 * w2;
+    den = (w1 - w2) * (w2 * (2.0 + 3.0 * w1) - 8.0 * w1);
+    a = (4.0 * w11 + 2.0 * w12 * (w1 - 6.0) + w22 * (w1 * (10.0 - 3.0 * w1) - 4.0)) / den;
+    b = (4.0 * w12 * (9.0 * w1 - 16.0) - 4.0 * w11 - 2.0 * w22 * (2.0 + 9.0 * w1 * (w1 - 2.0))) / (3.0 * den);
+    /* velocity-derivative estimates from the pre-collision second-order cumulants */
+    dx = -w1 / (2.0 * rho) * (2.0 * cmono[x2] - cmono[y2] - cmono[z2])
+         - w2 / (2.0 * rho) * (cmono[x2] + cmono[y2] + cmono[z2] - rho);
+    dy = dx + (3.0 * w1) / (2.0 * rho) * (cmono[x2] - cmono[y2]);
+    dz = dx + (3.0 * w1) / (2.0 * rho) * (cmono[x2] - cmono[z2]);
+    dxy = -3.0 * w1 / rho * cmono[xy];
+    dxz = -3.0 * w1 / rho * cmono[xz];
+    dyz = -3.0 * w1 / rho * cmono[yz];
+    g = 1.0 / w1 - 0.5;
+    cpost[kp[0]] += 2.0 / 3.0 * g * w6 * a * rho * (dx - 2.0 * dy + dz);
+    cpost[kp[1]] += 2.0 / 3.0 * g * w6 * a * rho * (dx + dy - 2.0 * dz);
+    cpost[kp[2]] += -4.0 / 3.0 * g * w7 * a * rho * (dx + dy + dz);
+    cpost[kp[3]] += -1.0 / 3.0 * g * w8 * b * rho * dyz;
+    cpost[kp[4]] += -1.0 / 3.0 * g * w8 * b * rho * dxz;
+    cpost[kp[5]] += -1.0 / 3.0 * g * w8 * b * rho * dxy;
+}
+
 static void collide_cumulant(const om_method* m, const double* f, double* fo, double* omega_out,
                              int all_rates_one) {
     int Q = m->Q, i, k, d, n;
@@ -520,6 +615,7 @@ static void collide_cumulant(const om_method* m, const double* f, double* fo, do
         cpost[kxz] += -3.0 * rho * (1.0 - o1 / 2.0) * (u[0] * u[0] * dx - u[2] * u[2] * dz);
         cpost[kb] += -3.0 * rho * (1.0 - o2 / 2.0) * (u[0] * u[0] * dx + u[1] * u[1] * dy + u[2] * u[2] * dz);
     }
+    if (m->foc_limiter > 0.0 && !all_rates_one) fourth_order_correction(m, rho, cmono, cpoly, cpost);
     for (n = 0; n < 27; ++n) {
         double s = 0.0;
         for (k = 0; k < Q; ++k) s += m->Minv[n][k] * cpost[k];
@@ -537,8 +633,55 @@ static void collide_cumulant(const om_method* m, const double* f, double* fo, do
     if (m->zero_centered) for (i = 0; i < Q; ++i) fo[i] -= m->w[i];
 }
 
+/* Central-moment method (D3Q27, compressible): polynomial central moments about the equilibrium
+ * velocity relaxed towards those of the continuous Maxwellian, forcing applied in central-moment
+ * space (methods/momentbased/centralmomentbasedmethod.py:296-394, relax_central_moments;
+ * forcemodels.py:201-203 Simple, :261-263 Luo, :300-306 Guo with (1 - omega/2)).  The equilibrium
+ * central moments are rho times those of a Gaussian of variance 1/3 (independent of u; the
+ * truncated raw Maxwellian moments give the same values, which tests/test_central_moment.py checks
+ * symbolically). */
+static void collide_central(const om_method* m, const double* f, double* fo) {
+    int Q = m->Q, i, k, n, d;
+    double rho, drho, rho_ref, u[3], km[27], kbg[27], keq[27], kf[27], post[27], mono[27], fpop[27] = {0};
+    static const double g[3] = {1.0, 0.0, 1.0 / 3.0};
+    conserved(m, f, &rho, &drho, &rho_ref, u);
+    if (m->force_model == 1)                      /* Guo: equilibrium velocity shift F / (2 rho) */
+        for (d = 0; d < 3; ++d) u[d] += m->F[d] / (2.0 * rho);
+    central_moments(m, f, u, km);
+    if (m->zero_centered) {
+        central_moments(m, m->w, u, kbg);
+        for (n = 0; n < 27; ++n) km[n] += kbg[n];
+    }
+    km[0] = rho;
+    for (n = 0; n < 27; ++n) keq[n] = rho * g[n / 9] * g[(n / 3) % 3] * g[n % 3];
+    for (n = 0; n < 27; ++n) kf[n] = 0.0;
+    if (m->force_model == 1 || m->force_model == 3 || m->force_model == 4) {
+        for (i = 0; i < Q; ++i) {
+            double cu = 0.0, cf = 0.0, t = 0.0;
+            for (d = 0; d < 3; ++d) { cu += m->c[i][d] * u[d]; cf += m->c[i][d] * m->F[d]; }
+            if (m->force_model == 3) t = 3.0 * cf;                        /* Simple */
+            else for (d = 0; d < 3; ++d) t += m->F[d] * ((m->c[i][d] - u[d]) * 3.0 + m->c[i][d] * cu * 9.0);
+            fpop[i] = m->w[i] * t;
+        }
+        central_moments(m, fpop, u, kf);
+    }
+    for (k = 0; k < Q; ++k) {
+        double pk = 0.0, pe = 0.0, pf = 0.0;
+        for (n = 0; n < 27; ++n) { pk += m->M[k][n] * km[n]; pe += m->M[k][n] * keq[n]; pf += m->M[k][n] * kf[n]; }
+        post[k] = pk + m->rate[k] * (pe - pk) + (m->force_model == 1 ? 1.0 - 0.5 * m->rate[k] : 1.0) * pf;
+    }
+    for (n = 0; n < 27; ++n) {
+        double s = 0.0;
+        for (k = 0; k < Q; ++k) s += m->Minv[n][k] * post[k];
+        mono[n] = s;
+    }
+    populations_from_central(m, mono, u, fo);
+    if (m->zero_centered) for (i = 0; i < Q; ++i) fo[i] -= m->w[i];
+}
+
 void om_collide(const om_method* m, const double* f, double* fo, double* omega_out) {
     if (m->kind == 1) collide_cumulant(m, f, fo, omega_out, 0);
+    else if (m->kind == 2) collide_central(m, f, fo);
     else collide_moment(m, f, fo, omega_out);
 }
 
@@ -548,7 +691,7 @@ void om_equilibrium(const om_method* m, double rho, const double uin[3], double*
     for (d = 0; d < 3; ++d) u[d] = uin[d];
     if (m->force_model != 0)                   /* macroscopic_velocity_shift, forcemodels.py:592 */
         for (d = 0; d < 3; ++d) u[d] -= m->F[d] / (2.0 * rho_ref);
-    if (m->kind == 1) {
+    if (m->kind == 1 || m->kind == 2) {      /* the Gaussian in central moments, shifted by u */
         double cc[27], mm[27], km[27];
         for (i = 0; i < 27; ++i) cc[i] = 0.0;
         cc[18] = cc[6] = cc[2] = 1.0 / 3.0;
@@ -650,11 +793,16 @@ void om_periodic_sync(const om_method* m, const om_grid* gr, int pattern, int pr
  * location lies beyond the ghost layer of a non-periodic axis. */
 static double f_out_at(const om_method* m, const om_grid* gr, const int periodic[3], int ooff[QMAX][3],
                        int oslot[QMAX], const double* f, int x, int y, int z, int d, int* ok) {
-    int c[3] = {x + ooff[d][0], y + ooff[d][1], z + ooff[d][2]}, a;
+    /* the sweep wrote from the interior image of the cell, at the write offset, into a ghost cell
+     * where that offset crosses a face: om_periodic_sync moves such values to the periodic image
+     * and copies them back, except in ghost cells beyond a non-periodic face (edges and corners),
+     * so the value is always found at the unwrapped write location of the wrapped cell */
+    int c[3] = {x, y, z}, a;
     for (a = 0; a < 3; ++a) {
         if (a >= m->D) continue;
         if (periodic[a]) c[a] = ((c[a] % gr->n[a]) + gr->n[a]) % gr->n[a];
-        else if (c[a] < -1 || c[a] > gr->n[a]) { *ok = 0; return 0.0; }
+        c[a] += ooff[d][a];
+        if (c[a] < -1 || c[a] > gr->n[a]) { *ok = 0; return 0.0; }
     }
     *ok = 1;
     return f[gidx(gr, c[0], c[1], c[2]) + oslot[d] * gr->s[3]];
@@ -825,6 +973,15 @@ void om_reduce(const om_method* m, const om_grid* gr, int pattern, int prev_pari
 }
 
 int om_sizeof_method(void) { return (int)sizeof(om_method); }
+
+/* Threads of the OpenMP loops that follow (small grids run faster on one thread). */
+void om_set_threads(int n) {
+#ifdef _OPENMP
+    omp_set_num_threads(n > 0 ? n : omp_get_num_procs());
+#else
+    (void)n;
+#endif
+}
 
 /* The accessor table of one pattern / parity: read (rw = 0) or write (rw = 1) offset off[3*i..]
  * and slot slot[i] of every direction i. */

@@ -54,6 +54,7 @@ class OmMethod(ctypes.Structure):
         ("fd_rho1", ctypes.c_double),
         ("link_code", ctypes.c_void_p),
         ("link_value", ctypes.c_void_p),
+        ("foc_limiter", ctypes.c_double),
     ]
 
 
@@ -151,6 +152,7 @@ class Oracle:
             assert w.size == MLP_NPARAM, f"closure parameters: {w.size} != {MLP_NPARAM}"
             ctypes.memmove(ctypes.addressof(m.mlp), w.ctypes.data, w.nbytes)
         m.discrete_eq = int(not method.continuous_equilibrium)
+        m.foc_limiter = float(method.fourth_order_limiter)
         self._m = m
         self.M = np.array([[float(v) for v in r] for r in M])
         self.Minv = np.array([[float(v) for v in r] for r in Minv])
@@ -235,6 +237,8 @@ class Oracle:
         SimpleExtrapolationOutflow, ExtrapolationOutflow, NoSlipLinearBouzidi with the per-link
         link_code [x, y, z, Q] and link_value [x, y, z, Q, 2] (the outflow state is updated in a copy)."""
         g = self._grid(f)
+        # small grids: the OpenMP fork per loop costs more than the loop
+        lib().om_set_threads(1 if g.n[0] * g.n[1] * g.n[2] < 32768 else 0)
         link = None
         if ubb_link is not None:
             link = np.ascontiguousarray(np.asarray(ubb_link, np.float64).transpose(2, 1, 0, 3, 4))
@@ -300,6 +304,52 @@ class Oracle:
                         fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if fl is not None else None,
                         self._ptr(out))
         return out
+
+
+    # -- sparse (list-based) domains --------------------------------------------------------
+    def sparse_ubb(self, flat, n_cells, links, velocity):
+        """lbmpy's UBB on a PDF list (the kernel SparseLbBoundaryMapper builds, sparse/mapping.py:157-247,
+        with boundaries/boundaryconditions.py UBB): for every link (dir d, fluid cell c, boundary cell
+        b), slot inv(d) of b receives f(c, d) - 6 w_d rho (c_d . u), rho the cell density when
+        compressible (zero-centred PDFs: 1 + sum f), else 1."""
+        dirs, w = self.spec.dirs, self.spec.weights
+        u = np.zeros(3)
+        u[:len(velocity)] = velocity
+        for d, c, b in links:
+            d, c, b = int(d), int(c), int(b)
+            if not 1 <= d < self.Q:
+                continue
+            rho = 1.0
+            if self.spec.compressible:
+                rho = float(sum(flat[c + i * n_cells] for i in range(self.Q)))
+                rho += 1.0 if self.spec.zero_centered else 0.0
+            inv = dirs.index(tuple(-v for v in dirs[d]))
+            cu = sum(dirs[d][k] * u[k] for k in range(self.D))
+            flat[b + inv * n_cells] = flat[c + d * n_cells] - 6.0 * float(w[d]) * cu * rho
+
+    def sparse_run(self, f, index, steps, ubb_links=None, ubb_velocity=(0.0, 0.0, 0.0)):
+        """lbmpy's sparse stream-pull-collide (sparse/update_rule_sparse.py:22-52 and the
+        substitutions of :115-125): f is a PDF list [n_cells, Q] (element (c, i) = PDF i of list cell
+        c), index the [n_fluid, Q - 1] pull index (sparse/mapping.py:100-156); each step cell c < n_fluid
+        gathers f(c, 0) and flat[index[c, i - 1]] for i >= 1, collides (om_collide) and writes its own
+        slots of the new list.  ubb_links [(dir, fluid cell, boundary cell)] run sparse_ubb on the
+        source list before each step.  Returns the new list (boundary cells keep their values)."""
+        n_cells, q = f.shape
+        n_fluid = index.shape[0]
+        flat = np.ascontiguousarray(np.asarray(f, np.float64).T).reshape(-1)
+        idx = np.asarray(index, np.int64)
+        for _ in range(steps):
+            if ubb_links is not None:
+                self.sparse_ubb(flat, n_cells, ubb_links, ubb_velocity)
+            gathered = np.empty((n_fluid, q))
+            gathered[:, 0] = flat[:n_fluid]
+            gathered[:, 1:] = flat[idx]
+            out = flat.copy()
+            for c in range(n_fluid):
+                fo = self.collide(gathered[c])
+                out[c + np.arange(q) * n_cells] = fo
+            flat = out
+        return flat.reshape(q, n_cells).T.copy()
 
 
 def make(stencil, method, **kw) -> Oracle:

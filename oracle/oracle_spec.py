@@ -311,7 +311,7 @@ def magic_rate(omega, magic=Fraction(3, 16)):
 # --------------------------------------------------------------------------------------------
 # The resolved method that the C oracle consumes
 # --------------------------------------------------------------------------------------------
-KIND_MOMENT, KIND_CUMULANT = 0, 1
+KIND_MOMENT, KIND_CUMULANT, KIND_CENTRAL = 0, 1, 2
 FORCE_NONE, FORCE_GUO, FORCE_CENTRAL_MOMENT, FORCE_SIMPLE, FORCE_LUO = 0, 1, 2, 3, 4
 SGS_NONE, SGS_SMAGORINSKY, SGS_MLP = 0, 1, 2
 
@@ -336,6 +336,7 @@ class OracleMethod:
     shear_rate: float = 0.0
     mlp: object = None            # learned-closure parameters (float32 array) when sgs == SGS_MLP
     continuous_equilibrium: bool = True   # SRT/TRT/MRT: False = discrete Maxwellian
+    fourth_order_limiter: float = 0.0     # > 0: fourth-order correction with this limiter
 
     @property
     def Q(self):
@@ -346,11 +347,28 @@ class OracleMethod:
         return len(self.dirs[0])
 
 
+def fourth_order_rates(w1: float, w2: float):
+    """Optimal third-order rates (w3, w4, w5) before the limiters and the parameters (a, b) of the
+    fourth-order correction for shear rate w1 and bulk rate w2 (Geier et al. 2017, eq. 111-116;
+    methods/cumulantbased/fourth_order_correction.py:79-97 and :149-170)."""
+    w11, w12, w22 = w1 * w1, w1 * w2, w2 * w2
+    w3 = (8 * (w1 - 2) * (w2 * (3 * w1 - 1) - 5 * w1)) / (
+        8 * (5 - 2 * w1) * w1 + w2 * (8 + w1 * (9 * w1 - 26)))
+    w4 = (8 * (w1 - 2) * (w1 + w2 * (3 * w1 - 7))) / (w2 * (56 - 42 * w1 + 9 * w11) - 8 * w1)
+    w5 = (24 * (w1 - 2) * (4 * w11 + w12 * (18 - 13 * w1) + w22 * (2 + w1 * (6 * w1 - 11)))) / (
+        16 * w11 * (w1 - 6) - 2 * w12 * (216 + 5 * w1 * (9 * w1 - 46))
+        + w22 * (w1 * (3 * w1 - 10) * (15 * w1 - 28) - 48))
+    den = (w1 - w2) * (w2 * (2 + 3 * w1) - 8 * w1)
+    a = (4 * w11 + 2 * w12 * (w1 - 6) + w22 * (w1 * (10 - 3 * w1) - 4)) / den
+    b = (4 * w12 * (9 * w1 - 16) - 4 * w11 - 2 * w22 * (2 + 9 * w1 * (w1 - 2))) / (3 * den)
+    return (w3, w4, w5), (a, b)
+
+
 def resolve(stencil: str, method: str, relaxation_rate=None, relaxation_rates=None,
             compressible=False, zero_centered=True, delta_equilibrium=None,
             equilibrium_order=2, force=(0.0, 0.0, 0.0), force_model=None,
             galilean_correction=False, smagorinsky=None, mlp=None,
-            continuous_equilibrium=True) -> OracleMethod:
+            continuous_equilibrium=True, fourth_order_correction=False) -> OracleMethod:
     """Follows ``LBMConfig.__post_init__`` (creationfunctions.py:347-484) and
     ``create_lb_method`` (creationfunctions.py:773-868) for SRT/TRT/MRT/CUMULANT."""
     method = method.lower()
@@ -365,6 +383,18 @@ def resolve(stencil: str, method: str, relaxation_rate=None, relaxation_rates=No
         else:
             relaxation_rates = [relaxation_rate]
     relaxation_rates = list(relaxation_rates)
+    foc_limiter = 0.0
+    if fourth_order_correction:
+        # creationfunctions.py:696-707 and :835-846: the method takes ten rates, the shear and bulk
+        # rates (bulk 1 by default), the optimal third-order rates and 1 for every higher group
+        if method != "cumulant" or stencil != "D3Q27":
+            raise ValueError("Fourth-order correction can only be applied to D3Q27 cumulant methods.")
+        if len(relaxation_rates) == 1:
+            relaxation_rates.append(1.0)
+        w1, w2 = float(relaxation_rates[0]), float(relaxation_rates[1])
+        (w3, w4, w5), _ = fourth_order_rates(w1, w2)
+        relaxation_rates = [w1, w2, w3, w4, w5, 1.0, 1.0, 1.0, 1.0, 1.0]
+        foc_limiter = 1e6 if fourth_order_correction is True else float(fourth_order_correction)
     if method == "cumulant" and not compressible:
         raise ValueError("Incompressible cumulant-based methods are not supported (yet).")
     if delta_equilibrium is None:
@@ -398,6 +428,19 @@ def resolve(stencil: str, method: str, relaxation_rate=None, relaxation_rates=No
         rates = [float(r) for _, r in info]
         kind = KIND_CUMULANT
         delta_equilibrium = False
+    elif method in ("central_moment", "centralmoment"):
+        # creationfunctions.py:818-822 -> methods/creationfunctions.py:336-381 with
+        # default_moment_sets.cascaded_moment_sets_literature (the D3Q27 groups equal the cumulants')
+        if stencil != "D3Q27":
+            raise ValueError("oracle central-moment method: D3Q27 only")
+        if not compressible:
+            raise ValueError("oracle central-moment method: compressible only")
+        nested = cumulant_groups_d3q27()
+        info = relaxation_info(relaxation_rates, nested, dim)
+        moments = [m for m, _ in info]
+        rates = [float(r) for _, r in info]
+        kind = KIND_CENTRAL
+        delta_equilibrium = False
     else:
         raise ValueError(method)
     if galilean_correction and (method != "cumulant" or stencil != "D3Q27"):
@@ -417,4 +460,5 @@ def resolve(stencil: str, method: str, relaxation_rate=None, relaxation_rates=No
                         equilibrium_order=equilibrium_order, force_model=fm, force=force,
                         galilean_correction=bool(galilean_correction), sgs=sgs, sgs_constant=c_sgs,
                         shear_rate=float(shear), mlp=mlp,
-                        continuous_equilibrium=bool(continuous_equilibrium) or kind != KIND_MOMENT)
+                        continuous_equilibrium=bool(continuous_equilibrium) or kind != KIND_MOMENT,
+                        fourth_order_limiter=foc_limiter)

@@ -7,8 +7,8 @@
 - c2: D3Q27 cumulant, Galilean-corrected, FP32, AA, 256 x 128 x 128 channel (NoSlip y/z walls,
   periodic x, CentralMoment force 1e-7, omega 1.95, seeded velocity noise 1e-4), 20000 steps; the
   axial velocity against the start-up solution of the rectangular duct (tests/analytic.py).
-- c3: D3Q19 TRT periodic Taylor-Green box stored in FP16 and BF16 (zero-centred, FP32 collision)
-  against the same run in FP64: relative L2 velocity error.
+- c3: D3Q19 TRT periodic Taylor-Green box stored in FP16, BF16 and e3m12 (zero-centred, FP32
+  collision) against the same run in FP64: relative L2 velocity error.
 - c4: the 512-cavity D3Q19 MRT batch (lid_driven_cavity_batch(512, seed=0)), 2000 steps in one
   persistent launch per step, eight seeded cavities against the same cavity run alone.
 """
@@ -87,7 +87,8 @@ def test_c2_channel_256x128x128_20000_steps_matches_duct_flow(cuda):
     assert np.isfinite(step.velocity_array).all()
 
 
-@pytest.mark.parametrize("storage,bound", [("float32", 1e-4), ("float16", 2e-3), ("bfloat16", 3e-2)])
+@pytest.mark.parametrize("storage,bound", [("float32", 1e-4), ("float16", 2e-3), ("bfloat16", 3e-2),
+                                           ("e3m12", 5e-4)])
 def test_c3_16bit_storage_error_against_fp64(cuda, storage, bound):
     from lbmpy_b200.precision import precision_study
     res = precision_study(128, 1000, 1000, storages=(storage,), device="cuda", log=lambda *_: None)

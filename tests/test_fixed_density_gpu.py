@@ -1,4 +1,4 @@
-"""FixedDensity outlets on the GPU (the pre-sweep k_fixed_density plus the sweep) against the FP64
+"""FixedDensity outlets on the GPU (the boundary pre-pass k_boundary_prepass plus the sweep) against the FP64
 oracle: velocity inlet, density outlet, no-slip channel walls; SRT/TRT, MRT and cumulant, pull
 and in-place patterns, FP64 and FP32 storage."""
 import numpy as np

@@ -120,3 +120,27 @@ def test_staged_not_used_where_it_does_not_apply(cuda, monkeypatch):
                                method=L.Method.TRT, relaxation_rate=1.7, streaming_pattern="esotwist",
                                config=L.CreateKernelConfig(data_type="float32"))
     assert s.sweep_variant() == "cell"
+
+
+def test_staged_wait_runs_out_and_reports(cuda, monkeypatch):
+    """lbm_plan_set_stage_wait: every CTA waits, before its last tile, on a barrier that nothing
+    arrives at; the wait runs out after 2 ms, the sweep sets LBM_STATUS_STAGE_TIMEOUT and returns
+    with that tile unswept.  The context stays usable: with the probe off the next sweeps complete
+    and match the oracle again from a fresh state."""
+    from lbmpy_b200 import _native as N
+    case = STAGED_CASES[0]
+    step, orc, f, flags, ubb, prev = _run_case(case, "float64", monkeypatch)
+    plan = step._bound().plan
+    N.check(N.lib().lbm_plan_set_stage_wait(plan.handle, 2_000_000, 1), "lbm_plan_set_stage_wait")
+    step.run(1)
+    torch.cuda.synchronize()
+    assert step.sweep_status() == N.STATUS_STAGE_TIMEOUT
+    assert step.sweep_status() == 0            # the read above cleared it
+    N.check(N.lib().lbm_plan_set_stage_wait(plan.handle, 0, 0), "lbm_plan_set_stage_wait")
+    with pytest.raises(ValueError):
+        N.check(N.lib().lbm_plan_set_stage_wait(plan.handle, 61 * 10 ** 9, 0), "lbm_plan_set_stage_wait")
+    name, stencil, method, pattern, n, periodic, bkind, kw = case
+    step2, orc2, f2, flags2, ubb2, prev2 = _run_case(case, "float64", monkeypatch)
+    res, _ = run_pair(step2, orc2, f2, flags2, ubb2, prev2, 20, pattern, periodic)
+    assert step2.sweep_status() == 0
+    assert pop_rel_linf(_interior(step2.pdfs), res[1:-1, 1:-1, 1:-1], step2.method.weights) < 1e-12
