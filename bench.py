@@ -37,10 +37,12 @@ METRIC = "D3Q19/D3Q27 GLUPS and % of HBM roofline; FP16-store vs FP32 at equal L
 # DRAM bytes (read + write) per sweep launch from one ncu capture of the same workload, averaged
 # over the launches captured; summaries with their commands are under profiles/.
 NCU_TRAFFIC_BYTES = {
-    "d3q27-cumulant-aa-channel-256x128x128": 875_081_216,   # k_sweep_d3q27_cumulant_aa_channel_256x128x128.md
-    "d3q19-trt-pull-float32-256": 2_547_412_000,            # k_sweep_d3q19_fp32_fp16_256.md
-    "d3q19-mrt-pull-float32-256": 2_550_143_000,
+    "d3q27-cumulant-aa-channel-256x128x128": 872_550_000,   # k_sweep_d3q27_cumulant_aa_channel_256x128x128.md
+    "d3q19-trt-pull-float32-256": 2_548_790_000,            # k_sweep_d3q19_fp32_fp16_256.md
+    "d3q19-mrt-pull-float32-256": 2_555_021_000,
     "d3q19-trt-pull-float16-256": 1_276_317_824,             # k_sweep_quad_d3q19_trt_pull_fp16_256.md
+    "d3q19-trt-pull-e3m12-256": 1_273_168_384,               # k_sweep_quad_d3q19_trt_pull_e3m12_256.md
+    "sparse-porous-192-d3q19-trt-float32": 996_429_312,      # k_sweep_sparse_porous_192_d3q19_trt_fp32.md
 }
 
 
@@ -398,7 +400,10 @@ def main():
 
     # roofline of the sweep kernel (the only kernel in the timed region)
     peak, peak_kind = measured_peak()
-    achieved = algorithmic_bytes_per_sweep(cells, q_pop, itemsize) / (ms / args.steps * 1e-3) / 1e9
+    bytes_per_sweep = algorithmic_bytes_per_sweep(cells, q_pop, itemsize)
+    if args.workload.startswith("sparse"):
+        bytes_per_sweep += 4 * (q_pop - 1) * cells          # the pull index of every fluid cell
+    achieved = bytes_per_sweep / (ms / args.steps * 1e-3) / 1e9
     traffic = NCU_TRAFFIC_BYTES.get(args.workload)
 
     # end to end through the public API: host PDFs in, run, PDFs and macroscopic fields out
@@ -518,7 +523,7 @@ def main():
                            else "inputs fit in L2 (no flush)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                             "bytes_per_lu": 2 * q_pop * itemsize},
+                             "bytes_per_lu": bytes_per_sweep / cells},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
                 "clocks": clocks.summary(), "secondary": secondary}
         if batched:

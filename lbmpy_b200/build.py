@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "liblbmb200.so")
 SOURCES = ["lbm_abi.cu", "lbm_q19_pop.cu", "lbm_q19_mrt.cu", "lbm_q27_pop.cu", "lbm_q27_mrt.cu",
            "lbm_q27_cum.cu", "lbm_q27_cum1.cu", "lbm_q27_cm.cu", "lbm_q27_closure.cu", "lbm_mlp.cu",
            "lbm_halo.cu", "lbm_q19_pop_b.cu", "lbm_q19_mrt_b.cu", "lbm_q27_pop_b.cu", "lbm_q27_cum_b.cu",
-           "lbm_q27_cum1_b.cu"]
+           "lbm_q27_cum1_b.cu", "lbm_q27_mrt_b.cu", "lbm_q27_cm_b.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -73,6 +73,15 @@ def generate() -> str:
         out.append(_array_fn(pre + "mrt_M", [_f(v) for r in Mm for v in r], nidx=2, dims=(q, q)))
         out.append(_array_fn(pre + "mrt_Minv", [_f(v) for r in Minv for v in r], nidx=2, dims=(q, q)))
         out.append(_array_fn(pre + "mrt_p0", [_f(e[0]) for e in eq]))
+        # moments of the Luo / Guo force populations w_i (9 (c.F)(c.u) + 3 c.F - 3 u.F): for an even
+        # row, 9 sum_ab T_k,ab F_a u_b - 3 (u.F) S_k; for an odd row, 3 sum_a B_k,a F_a
+        prs = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
+        T = [[sum(Mm[k][i] * w[i] * dirs[i][a] * dirs[i][b] for i in range(q)) for a, b in prs] for k in range(q)]
+        B = [[sum(Mm[k][i] * w[i] * dirs[i][a] for i in range(q)) for a in range(3)] for k in range(q)]
+        S = [sum(Mm[k][i] * w[i] for i in range(q)) for k in range(q)]
+        out.append(_array_fn(pre + "mrt_fT", [_f(v) for r in T for v in r], nidx=2, dims=(q, 6)))
+        out.append(_array_fn(pre + "mrt_fB", [_f(v) for r in B for v in r], nidx=2, dims=(q, 3)))
+        out.append(_array_fn(pre + "mrt_fS", [_f(v) for v in S]))
         out.append(_array_fn(pre + "mrt_lin", [_f(v) for e in eq for v in e[1]], nidx=2, dims=(q, 3)))
         out.append(_array_fn(pre + "mrt_quad", [_f(v) for e in eq for v in e[2]], nidx=2, dims=(q, 6)))
         out.append("")

@@ -157,44 +157,41 @@ __device__ __forceinline__ R collide_mrt(R (&f)[Q], const Physics& p) {
     const R rf = p.compressible ? m.rho : R(1);
     const R uu[6] = {m.ux * m.ux, m.uy * m.uy, m.uz * m.uz, m.ux * m.uy, m.ux * m.uz, m.uy * m.uz};
     const bool has_force = p.force_model == FM_GUO || p.force_model == FM_SIMPLE || p.force_model == FM_LUO;
-    R luo[Q];
-    if (has_force) {
-        const R Fx = R(p.force[0]), Fy = R(p.force[1]), Fz = R(p.force[2]);
-        const R uF = m.ux * Fx + m.uy * Fy + m.uz * Fz;
-#pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
-            const R cu = R(L::cx(i)) * m.ux + R(L::cy(i)) * m.uy + R(L::cz(i)) * m.uz;
-            luo[i] = p.force_model == FM_SIMPLE ? R(L::w(i)) * R(3) * cF
-                                                : R(L::w(i)) * (R(9) * cF * cu + R(3) * cF - R(3) * uF);
-        }
-    }
+    // Moments of the force populations (Luo and Guo: w_i (9 (c.F)(c.u) + 3 c.F - 3 u.F); Simple:
+    // 3 w_i c.F) in closed form: the even rows see 9 sum_ab T_ab F_a u_b - 3 (u.F) S, the odd rows
+    // 3 sum_a B_a F_a (tables generated from the basis).
+    const R Fx = R(p.force[0]), Fy = R(p.force[1]), Fz = R(p.force[2]);
+    const bool simple = p.force_model == FM_SIMPLE;
+    const R FU[6] = {Fx * m.ux, Fy * m.uy, Fz * m.uz, Fx * m.uy + Fy * m.ux, Fx * m.uz + Fz * m.ux,
+                     Fy * m.uz + Fz * m.uy};
+    const R uF = m.ux * Fx + m.uy * Fy + m.uz * Fz;
     // Every row of the weighted-orthogonal basis is even or odd under c -> -c, so the transforms
-    // run on the sums and differences of opposite populations, f_i +- f_inv(i): half the terms
-    // of the dense Q x Q products.
+    // run on the sums and differences of opposite populations, f_i +- f_inv(i): half the terms of
+    // the dense Q x Q products.  The moment changes are folded into the even and odd parts of the
+    // result as soon as they are known, so no array of them stays live.
     constexpr int NP = (Q - 1) / 2;
-    R fs[NP], fd[NP], ls[NP], ld[NP];
+    R fs[NP], fd[NP], ev[NP], od[NP];
+    const R f0 = f[0];
 #pragma unroll
-    for (int p2 = 0; p2 < NP; ++p2) {
-        const int i = L::pair(p2), j = L::inv(L::pair(p2));
-        fs[p2] = f[i] + f[j];
-        fd[p2] = f[i] - f[j];
-        if (has_force) {
-            ls[p2] = luo[i] + luo[j];
-            ld[p2] = luo[i] - luo[j];
-        }
+    for (int q2 = 0; q2 < NP; ++q2) {
+        const int i = L::pair(q2), j = L::inv(L::pair(q2));
+        fs[q2] = f[i] + f[j];
+        fd[q2] = f[i] - f[j];
+        ev[q2] = R(0);
+        od[q2] = R(0);
     }
-    R delta[Q];
+    R e0 = R(0);
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
+        const bool even = L::Meven(k);
         R mk = 0;
-        if (L::Meven(k)) {
-            mk = cmad(mk, L::M(k, 0), f[0]);
+        if (even) {
+            mk = cmad(mk, L::M(k, 0), f0);
 #pragma unroll
-            for (int p2 = 0; p2 < NP; ++p2) mk = cmad(mk, L::M(k, L::pair(p2)), fs[p2]);
+            for (int q2 = 0; q2 < NP; ++q2) mk = cmad(mk, L::M(k, L::pair(q2)), fs[q2]);
         } else {
 #pragma unroll
-            for (int p2 = 0; p2 < NP; ++p2) mk = cmad(mk, L::M(k, L::pair(p2)), fd[p2]);
+            for (int q2 = 0; q2 < NP; ++q2) mk = cmad(mk, L::M(k, L::pair(q2)), fd[q2]);
         }
         R lin = 0, quad = 0;
         lin = cmad(lin, L::mlin(k, 0), m.ux);
@@ -208,39 +205,37 @@ __device__ __forceinline__ R collide_mrt(R (&f)[Q], const Physics& p) {
         R d = r * (meq - mk);
         if (has_force) {
             R fk = 0;
-            if (L::Meven(k)) {
-                fk = cmad(fk, L::M(k, 0), luo[0]);
+            if (even) {
+                if (!simple) {
 #pragma unroll
-                for (int p2 = 0; p2 < NP; ++p2) fk = cmad(fk, L::M(k, L::pair(p2)), ls[p2]);
+                    for (int a = 0; a < 6; ++a) fk = cmad(fk, 9.0 * L::fT(k, a), FU[a]);
+                    fk = cmad(fk, -3.0 * L::fS(k), uF);
+                }
             } else {
-#pragma unroll
-                for (int p2 = 0; p2 < NP; ++p2) fk = cmad(fk, L::M(k, L::pair(p2)), ld[p2]);
+                fk = cmad(fk, 3.0 * L::fB(k, 0), Fx);
+                fk = cmad(fk, 3.0 * L::fB(k, 1), Fy);
+                fk = cmad(fk, 3.0 * L::fB(k, 2), Fz);
             }
             if (p.force_model == FM_GUO) fk *= (R(1) - R(0.5) * r);
             d += fk;
         }
-        delta[k] = d;
-    }
-    // back: column k of M^-1 is even or odd with row k of M, so f_i and f_inv(i) receive the even
-    // part plus or minus the odd part
-    {
-        R e0 = 0;
+        // back: column k of M^-1 is even or odd with row k of M, so f_i and f_inv(i) receive the
+        // even part plus or minus the odd part
+        if (even) {
+            e0 = cmad(e0, L::Minv(0, k), d);
 #pragma unroll
-        for (int k = 0; k < Q; ++k)
-            if (L::Meven(k)) e0 = cmad(e0, L::Minv(0, k), delta[k]);
-        f[0] += e0;
-    }
+            for (int q2 = 0; q2 < NP; ++q2) ev[q2] = cmad(ev[q2], L::Minv(L::pair(q2), k), d);
+        } else {
 #pragma unroll
-    for (int p2 = 0; p2 < NP; ++p2) {
-        const int i = L::pair(p2);
-        R e = 0, o = 0;
-#pragma unroll
-        for (int k = 0; k < Q; ++k) {
-            if (L::Meven(k)) e = cmad(e, L::Minv(i, k), delta[k]);
-            else o = cmad(o, L::Minv(i, k), delta[k]);
+            for (int q2 = 0; q2 < NP; ++q2) od[q2] = cmad(od[q2], L::Minv(L::pair(q2), k), d);
         }
-        f[i] += e + o;
-        f[L::inv(i)] += e - o;
+    }
+    f[0] = f0 + e0;
+#pragma unroll
+    for (int q2 = 0; q2 < NP; ++q2) {
+        const int i = L::pair(q2), j = L::inv(L::pair(q2));
+        f[i] += ev[q2] + od[q2];
+        f[j] += ev[q2] - od[q2];
     }
     return p.sgs == 1 ? om_sgs : R(0);
 }

@@ -74,6 +74,9 @@ template <> struct Lat<19> {
     }
     LBM_HD static constexpr double M(int k, int i) { return lbm_tables::q19_mrt_M(k, i); }
     LBM_HD static constexpr bool Meven(int k) { return lbm_tables::q19_mrt_even(k) != 0; }
+    LBM_HD static constexpr double fT(int k, int a) { return lbm_tables::q19_mrt_fT(k, a); }
+    LBM_HD static constexpr double fB(int k, int a) { return lbm_tables::q19_mrt_fB(k, a); }
+    LBM_HD static constexpr double fS(int k) { return lbm_tables::q19_mrt_fS(k); }
     LBM_HD static constexpr double Minv(int i, int k) { return lbm_tables::q19_mrt_Minv(i, k); }
     LBM_HD static constexpr double p0(int k) { return lbm_tables::q19_mrt_p0(k); }
     LBM_HD static constexpr double mlin(int k, int a) { return lbm_tables::q19_mrt_lin(k, a); }
@@ -96,6 +99,9 @@ template <> struct Lat<27> {
     }
     LBM_HD static constexpr double M(int k, int i) { return lbm_tables::q27_mrt_M(k, i); }
     LBM_HD static constexpr bool Meven(int k) { return lbm_tables::q27_mrt_even(k) != 0; }
+    LBM_HD static constexpr double fT(int k, int a) { return lbm_tables::q27_mrt_fT(k, a); }
+    LBM_HD static constexpr double fB(int k, int a) { return lbm_tables::q27_mrt_fB(k, a); }
+    LBM_HD static constexpr double fS(int k) { return lbm_tables::q27_mrt_fS(k); }
     LBM_HD static constexpr double Minv(int i, int k) { return lbm_tables::q27_mrt_Minv(i, k); }
     LBM_HD static constexpr double p0(int k) { return lbm_tables::q27_mrt_p0(k); }
     LBM_HD static constexpr double mlin(int k, int a) { return lbm_tables::q27_mrt_lin(k, a); }

@@ -306,7 +306,7 @@ MacroLauncher pick_set_eq_pattern(int pat) {
 
 // Reduced family (FP64 / FP32 storage, pull and AA): for bases whose fully unrolled 27x27
 // transforms make every extra instantiation expensive to compile.
-#define LBM_DEFINE_FAMILY_REDUCED(NAME, Q, MK)                                                  \
+#define LBM_DEFINE_FAMILY_REDUCED_A(NAME, Q, MK)                                              \
     template <class S, class R>                                                                 \
     static SweepLauncher NAME##_sweep_pat(int pat) {                                            \
         switch (pat) {                                                                          \
@@ -336,15 +336,6 @@ MacroLauncher pick_set_eq_pattern(int pat) {
         if (store == ST_F32) return pick_prepass_pattern<float, float, Q, MK>(pat);       \
         return nullptr;                                                                         \
     }                                                                                           \
-    StagedLauncher sweep_staged_##NAME(int store, int pat) {                                    \
-        if (store == ST_F64) return pick_staged_pattern<double, double, Q, MK>(pat);            \
-        if (store == ST_F32) return pick_staged_pattern<float, float, Q, MK>(pat);              \
-        return nullptr;                                                                         \
-    }                                                                                           \
-    SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
-        if (store == ST_F32) return pick_pair_pattern<float, Q, MK>(pat);                       \
-        return nullptr;                                                                         \
-    }                                                                                           \
     SweepLauncher sweep_##NAME(int store, int pat) {                                            \
         if (store == ST_F64) return NAME##_sweep_pat<double, double>(pat);                      \
         if (store == ST_F32) return NAME##_sweep_pat<float, float>(pat);                        \
@@ -363,6 +354,17 @@ MacroLauncher pick_set_eq_pattern(int pat) {
     MacroLauncher set_eq_##NAME(int store, int pat) {                                           \
         if (store == ST_F64) return NAME##_set_pat<double, double>(pat);                        \
         if (store == ST_F32) return NAME##_set_pat<float, double>(pat);                          \
+        return nullptr;                                                                         \
+    }
+
+#define LBM_DEFINE_FAMILY_REDUCED_B(NAME, Q, MK)                                              \
+    StagedLauncher sweep_staged_##NAME(int store, int pat) {                                    \
+        if (store == ST_F64) return pick_staged_pattern<double, double, Q, MK>(pat);            \
+        if (store == ST_F32) return pick_staged_pattern<float, float, Q, MK>(pat);              \
+        return nullptr;                                                                         \
+    }                                                                                           \
+    SweepLauncher sweep_pair_##NAME(int store, int pat) {                                       \
+        if (store == ST_F32) return pick_pair_pattern<float, Q, MK>(pat);                       \
         return nullptr;                                                                         \
     }
 

@@ -221,7 +221,8 @@ template <class S, int Q, int MK, int PAT> struct SweepMinBlocks { static conste
 template <> struct SweepMinBlocks<float, 27, MK_CUM1, PAT_AA_ODD> { static constexpr int value = 3; };
 template <> struct SweepMinBlocks<float, 27, MK_CUM1, PAT_AA_EVEN> { static constexpr int value = 4; };
 template <> struct SweepMinBlocks<float, 19, MK_POP, PAT_PULL> { static constexpr int value = 5; };
-template <> struct SweepMinBlocks<float, 19, MK_MRT, PAT_PULL> { static constexpr int value = 3; };
+template <> struct SweepMinBlocks<float, 19, MK_MRT, PAT_PULL> { static constexpr int value = 4; };
+template <> struct SweepMinBlocks<float, 27, MK_MRT, PAT_PULL> { static constexpr int value = 3; };
 
 template <class S, class R, int Q, int MK, int PAT>
 __global__ void __launch_bounds__(256, SweepMinBlocks<S, Q, MK, PAT>::value) k_sweep(const SweepArgs a) {
@@ -312,7 +313,7 @@ struct BatchArgs {
 };
 
 template <class S, class R, int Q, int MK, int PAT>
-__global__ void __launch_bounds__(256, 2) k_sweep_batched(const BatchArgs b) {
+__global__ void __launch_bounds__(256, 3) k_sweep_batched(const BatchArgs b) {
     __shared__ __align__(16) SweepArgs sa;
     constexpr int WORDS = sizeof(SweepArgs) / 4;
     static_assert(sizeof(SweepArgs) % 4 == 0, "SweepArgs is copied as 32-bit words");

@@ -238,7 +238,7 @@ class Oracle:
         link_code [x, y, z, Q] and link_value [x, y, z, Q, 2] (the outflow state is updated in a copy)."""
         g = self._grid(f)
         # small grids: the OpenMP fork per loop costs more than the loop
-        lib().om_set_threads(1 if g.n[0] * g.n[1] * g.n[2] < 32768 else 0)
+        lib().om_set_threads(1 if g.n[0] * g.n[1] * g.n[2] < 4096 else 0)
         link = None
         if ubb_link is not None:
             link = np.ascontiguousarray(np.asarray(ubb_link, np.float64).transpose(2, 1, 0, 3, 4))
