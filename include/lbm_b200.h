@@ -126,14 +126,17 @@ int lbm_sweep(const LbmPlan* plan, const void* src, void* dst, const int64_t str
 int lbm_plan_status(LbmPlan* plan, uint32_t* status, int clear);
 
 /* Which kernel lbm_sweep runs for these arguments: one cell per thread, two or four x-adjacent
- * cells per thread, or the row-staged sweep (shared-memory stages filled by bulk copies).  All
- * give lbmpy's update; the choice follows storage type, method, alignment and the environment
- * overrides LBM_B200_PAIR / LBM_B200_QUAD / LBM_B200_STAGED ("0" never, "1" when applicable).
+ * cells per thread, the row-staged sweep (shared-memory stages filled by bulk copies), or the
+ * pipelined z-column sweep (a column of cells per thread, the next cell's loads in flight during
+ * the current collision; D3Q27 cumulant FP32).  All give lbmpy's update; the choice follows
+ * storage type, method, alignment and the environment overrides LBM_B200_PAIR / LBM_B200_QUAD /
+ * LBM_B200_STAGED ("0" never, "1" when applicable) and LBM_B200_ZPIPE (cells per thread, >= 2).
  * Diagnostic: lbmpy has one generated kernel per configuration and no such query. */
 #define LBM_VARIANT_CELL 0
 #define LBM_VARIANT_PAIR 1
 #define LBM_VARIANT_QUAD 2
 #define LBM_VARIANT_STAGED 3
+#define LBM_VARIANT_ZPIPE 4
 int lbm_sweep_variant(const LbmPlan* plan, const void* src, const void* dst, const int64_t strides[4],
                       int parity, const float* omega_out, int* variant);
 

@@ -18,8 +18,8 @@ PATTERN_PULL, PATTERN_AA, PATTERN_ESOTWIST, PATTERN_PUSH, PATTERN_ESOPULL, PATTE
 FORCE_NONE, FORCE_GUO, FORCE_CENTRAL_MOMENT, FORCE_SIMPLE, FORCE_LUO = 0, 1, 2, 3, 4
 SGS_NONE, SGS_SMAGORINSKY, SGS_MLP = 0, 1, 2
 STATUS_STAGE_TIMEOUT = 1
-VARIANT_CELL, VARIANT_PAIR, VARIANT_QUAD, VARIANT_STAGED = 0, 1, 2, 3
-VARIANT_NAMES = {0: "cell", 1: "pair", 2: "quad", 3: "staged"}
+VARIANT_CELL, VARIANT_PAIR, VARIANT_QUAD, VARIANT_STAGED, VARIANT_ZPIPE = 0, 1, 2, 3, 4
+VARIANT_NAMES = {0: "cell", 1: "pair", 2: "quad", 3: "staged", 4: "zpipe"}
 MLP_PARAMS = 1442
 
 # exported symbols, one per declaration in include/lbm_b200.h

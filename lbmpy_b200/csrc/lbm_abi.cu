@@ -28,6 +28,7 @@ struct LbmPlan {
     int use_quad;          // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_QUAD)
     int use_staged;        // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_STAGED)
     int ns;                // shared-memory stages of the staged sweep (environment LBM_B200_NS, else 2)
+    int zpipe;             // cells per thread of the pipelined z-column sweep, 0 off (environment LBM_B200_ZPIPE)
     int sms;               // multiprocessors of the plan's device
     unsigned* status;      // device status word (lbm_plan_status), inside the reduction scratch
     uint32_t* rowmask;     // row summary of the flag field last finalized with this plan
@@ -658,6 +659,10 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
         if (p->zc < 1) p->zc = 1;
         const char* senv = getenv("LBM_B200_STAGED");
         p->use_staged = senv == nullptr ? -1 : (senv[0] == '0' ? 0 : 1);
+        const char* penv = getenv("LBM_B200_ZPIPE");
+        p->zpipe = penv != nullptr ? atoi(penv) : 0;
+        if (p->zpipe < 2) p->zpipe = 0;
+        if (p->zpipe > 64) p->zpipe = 64;
         const char* nenv = getenv("LBM_B200_NS");
         p->ns = nenv != nullptr ? atoi(nenv) : 2;
         if (p->ns < 2) p->ns = 2;
@@ -745,8 +750,14 @@ static int validate_sweep(const LbmPlan* p, const void* src, const void* dst, co
 }
 
 // Which sweep kernel a launch with these arguments uses (LBM_VARIANT_*), in order of preference.
+static bool zpipe_applicable(const LbmPlan* p, int pat, const float* omega_out) {
+    return p->zpipe >= 2 && p->mk == MK_CUM1 && p->store == ST_F32 && omega_out == nullptr &&
+           (pat == PAT_PULL || pat == PAT_AA_EVEN || pat == PAT_AA_ODD);
+}
+
 static int sweep_variant(const LbmPlan* p, const void* src, const void* dst, const int64_t strides[4], int pat,
                          const float* omega_out) {
+    if (zpipe_applicable(p, pat, omega_out)) return LBM_VARIANT_ZPIPE;
     if (staged_applicable(p, src, strides, pat)) return LBM_VARIANT_STAGED;
     if (quad_applicable(p, src, dst, strides, pat, omega_out)) return LBM_VARIANT_QUAD;
     if (pair_applicable(p, src, dst, strides, pat, omega_out)) return LBM_VARIANT_PAIR;
@@ -804,6 +815,10 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
         L = quad_launcher(p, pat);
         block = dim3(32, QUAD_ROWS, 1);
         grid = dim3((a.g.nx + 127) / 128, (a.g.ny + QUAD_ROWS - 1) / QUAD_ROWS, a.g.nz);
+    } else if (variant == LBM_VARIANT_ZPIPE) {
+        L = sweep_zpipe_q27_cum1(p->store, pat);
+        a.zc = p->zpipe;
+        launch_shape(a.g, a.zc, grid, block);
     } else if (variant == LBM_VARIANT_PAIR) {
         L = pair_launcher(p, pat);
         block = dim3(32, PAIR_ROWS, 1);

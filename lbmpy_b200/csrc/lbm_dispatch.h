@@ -118,6 +118,12 @@ cudaError_t launch_sparse_set(const SparseArgs& a, const double* rho, const doub
     return cudaGetLastError();
 }
 
+template <class S, class R, int Q, int MK, int PAT>
+cudaError_t launch_sweep_zpipe(const SweepArgs& a, dim3 grid, dim3 block, cudaStream_t s) {
+    k_sweep_zpipe<S, R, Q, MK, PAT><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 using BatchLauncher = cudaError_t (*)(const BatchArgs&, dim3, dim3, cudaStream_t);
 
 template <class S, class R, int Q, int MK, int PAT>
@@ -386,6 +392,9 @@ LBM_DECLARE_FAMILY(q27_mrt)
 LBM_DECLARE_FAMILY(q27_cum)
 LBM_DECLARE_FAMILY(q27_cum1)
 LBM_DECLARE_FAMILY(q27_cm)
+
+// Pipelined z-column sweep of the D3Q27 cumulant (orders >= 3 relaxed by 1), FP32, pull and AA.
+SweepLauncher sweep_zpipe_q27_cum1(int store, int pat);
 
 // error reporting shared by the entry points of every translation unit (lbm_abi.cu)
 int abi_fail(int code, const char* fmt, ...);

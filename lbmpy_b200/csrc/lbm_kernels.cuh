@@ -233,6 +233,58 @@ __global__ void __launch_bounds__(256, SweepMinBlocks<S, Q, MK, PAT>::value) k_s
     sweep_cell<S, R, Q, MK, PAT>(a, x, y, z);
 }
 
+// Pipelined z-columns: each thread sweeps a.zc consecutive cells along z and issues the loads of
+// the next cell before it collides the current one, so every warp keeps Q loads in flight through
+// its collision (the one-cell sweep has none in flight while it computes).  The second set of Q
+// values costs registers: two 256-thread blocks per SM.  Safe in place for AA: the locations a
+// cell reads and the locations it writes are the same set, disjoint from every other cell's.
+template <class S, class R, int Q, int MK, int PAT>
+__global__ void __launch_bounds__(256, 2) k_sweep_zpipe(const SweepArgs a) {
+    static_assert(PAT == PAT_PULL || PAT == PAT_AA_EVEN || PAT == PAT_AA_ODD, "pipelined sweep: pull and AA");
+    using A = Access<PAT>;
+    const Grid& g = a.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z0 = blockIdx.z * a.zc;
+    if (x >= g.nx || y >= g.ny || z0 >= g.nz) return;
+    const int z1 = min(z0 + a.zc, g.nz);
+    const S* src = static_cast<const S*>(a.src);
+    S* dst = static_cast<S*>(a.dst);
+    auto load = [&](int z, R (&h)[Q], int& hf) {
+        hf = (g.flags != nullptr && row_flagged(g, y, z)) ? g.flags[(x + 1) + (y + 1) * g.fsy + (z + 1) * g.fsz] : 0;
+        NbrOffsets nb;
+        nb.init(g, x, y, z);
+        const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int off = nb.off(A::template roff<Q>(i, 0), A::template roff<Q>(i, 1), A::template roff<Q>(i, 2));
+            h[i] = Conv<S, R>::ld(src + eidx(A::template rslot<Q>(i) * g.sq, cell + off));
+        }
+    };
+    R nxt[Q];
+    int nfl;
+    load(z0, nxt, nfl);
+#pragma unroll 1
+    for (int z = z0; z < z1; ++z) {
+        R f[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = nxt[i];
+        const int fl = nfl;
+        if (z + 1 < z1) load(z + 1, nxt, nfl);
+        if (fl & FLAG_TYPE_MASK) continue;
+        NbrOffsets nb;
+        nb.init(g, x, y, z);
+        const int cell = (x + 1) + (y + 1) * g.sy + (z + 1) * g.sz;
+        if (fl & FLAG_NEAR_WALL) bounce_back<S, R, Q, PAT>(f, a, nb, cell, x, y, z);
+        collide<R, Q, MK>(f, a.p);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int off = nb.off(A::template woff<Q>(i, 0), A::template woff<Q>(i, 1), A::template woff<Q>(i, 2));
+            Conv<S, R>::st(dst + eidx(A::template wslot<Q>(i) * g.sq, cell + off), f[i]);
+        }
+    }
+}
+
 // Asks L2 for the lines one cell will pull (prefetch.global.L2 is a hint: no data returns, no
 // registers are held, and every address is one the sweep itself reads).
 template <class S, int Q, int PAT>

@@ -118,17 +118,24 @@ def _boundaries(kind):
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("dtype,kernel", [("float64", "cell"), ("float32", "pair"), ("float32", "cell")])
+@pytest.mark.parametrize("dtype,kernel", [("float64", "cell"), ("float32", "pair"), ("float32", "cell"),
+                                          ("float32", "zpipe")])
 def test_sweep_parity(cuda, case, dtype, kernel, monkeypatch):
     """kernel='pair': two cells per thread with packed FP32x2 arithmetic (the default for even nx);
-    kernel='cell': one cell per thread (forced with LBM_B200_PAIR=0)."""
+    kernel='cell': one cell per thread (forced with LBM_B200_PAIR=0); kernel='zpipe': columns of
+    3 cells along z per thread with the next cell's loads in flight (D3Q27 cumulant FP32 only;
+    the other methods fall back to the one-cell sweep)."""
     name, stencil, method, pattern, n, periodic, bkind, kw = case
     monkeypatch.setenv("LBM_B200_PAIR", "1" if kernel == "pair" else "0")
+    if kernel == "zpipe":
+        monkeypatch.setenv("LBM_B200_ZPIPE", "3")
     if dtype == "float32" and stencil == "D3Q27" and method == "mrt" and pattern not in ("pull", "aa"):
         pytest.skip("not built")
     steps = 100
     step, orc, f, flags, ubb, prev = make_pair(stencil, method, n, pattern, dtype, periodic=periodic,
                                                boundaries=_boundaries(bkind), **kw)
+    if kernel == "zpipe" and method == "cumulant" and pattern in ("pull", "aa"):
+        assert step.sweep_variant() == "zpipe"
     # the setter first
     fluid0 = np.ones(n, bool) if bkind is None else \
         ((step.boundary_handling.flag_array & 7)[1:-1, 1:-1, 1:-1] == 0)
