@@ -95,9 +95,15 @@ class LatticeBoltzmannStep:
         self.pdfs = create_pdf_array(domain_size, q, dtype=self._storage, device=device)
         self.pdfs_tmp = None if self._inplace else create_pdf_array(domain_size, q, dtype=self._storage,
                                                                       device=device)
-        np_dt = np.float64 if self._compute == "float64" else np.float32
-        self._velocity = np.zeros(domain_size + (3,), dtype=np_dt)
-        self._density = np.ones(domain_size, dtype=np_dt)
+        # host density and velocity (lbmpy's CPU arrays of the step) live in page-locked memory, so
+        # that the copies of set_pdf_fields_from_macroscopic_values() and post_run() go by DMA; the
+        # numpy arrays are views of it
+        td = torch.float64 if self._compute == "float64" else torch.float32
+        pin = torch.cuda.is_available()
+        self._velocity_t = torch.zeros(tuple(domain_size) + (3,), dtype=td, pin_memory=pin)
+        self._density_t = torch.ones(tuple(domain_size), dtype=td, pin_memory=pin)
+        self._velocity = self._velocity_t.numpy()
+        self._density = self._density_t.numpy()
         self._boundary_handling = LatticeBoltzmannBoundaryHandling(self.method, domain_size, self.periodicity,
                                                                    name=name + "_boundary_handling", device=device,
                                                                    streaming_pattern=self.streaming_pattern)
@@ -226,8 +232,8 @@ class LatticeBoltzmannStep:
         return self._bound_sweep
 
     def set_pdf_fields_from_macroscopic_values(self):
-        rho = torch.from_numpy(np.ascontiguousarray(self._density)).to(self.device)
-        u = torch.from_numpy(np.ascontiguousarray(self._velocity)).to(self.device)
+        rho = self._density_t.to(self.device)
+        u = self._velocity_t.to(self.device)
         set_equilibrium(self._macro, self.pdfs, rho, u, self._prev, self.kernel_params, self.periodicity)
 
     def pre_run(self):
@@ -266,8 +272,8 @@ class LatticeBoltzmannStep:
         rho = torch.empty(self._domain, dtype=cd, device=self.device)
         u = torch.empty(self._domain + (3,), dtype=cd, device=self.device)
         get_macroscopic(self._macro, self.pdfs, rho, u, self._prev, self.kernel_params, self.periodicity)
-        self._density[...] = rho.cpu().numpy()
-        self._velocity[...] = u.cpu().numpy()
+        self._density_t.copy_(rho)
+        self._velocity_t.copy_(u)
 
     def run(self, time_steps):
         self.pre_run()
