@@ -29,6 +29,7 @@ struct LbmPlan {
     int use_staged;        // -1 default policy, 0 never, 1 whenever applicable (environment LBM_B200_STAGED)
     int ns;                // shared-memory stages of the staged sweep (environment LBM_B200_NS, else 2)
     int zpipe;             // cells per thread of the pipelined z-column sweep, 0 off (environment LBM_B200_ZPIPE)
+    int block_x;           // x extent of the one-cell sweep's 256-thread blocks, 0 automatic (LBM_B200_BX)
     int sms;               // multiprocessors of the plan's device
     unsigned* status;      // device status word (lbm_plan_status), inside the reduction scratch
     uint32_t* rowmask;     // row summary of the flag field last finalized with this plan
@@ -659,6 +660,9 @@ int lbm_plan_create(const LbmPlanDesc* desc, LbmPlan** out) {
         if (p->zc < 1) p->zc = 1;
         const char* senv = getenv("LBM_B200_STAGED");
         p->use_staged = senv == nullptr ? -1 : (senv[0] == '0' ? 0 : 1);
+        const char* benv = getenv("LBM_B200_BX");
+        p->block_x = benv != nullptr ? atoi(benv) : 0;
+        if (p->block_x != 32 && p->block_x != 64 && p->block_x != 128 && p->block_x != 256) p->block_x = 0;
         const char* penv = getenv("LBM_B200_ZPIPE");
         p->zpipe = penv != nullptr ? atoi(penv) : 0;
         if (p->zpipe < 2) p->zpipe = 0;
@@ -826,6 +830,10 @@ static int launch_sweep_checked(const LbmPlan* p, const void* src, void* dst, co
     } else {
         L = sweep_launcher(p, pat);
         launch_shape(a.g, a.zc, grid, block);
+        if (p->block_x > 0 && a.zc == 1) {
+            block = dim3(p->block_x, 256 / p->block_x, 1);
+            grid = dim3((a.g.nx + block.x - 1) / block.x, (a.g.ny + block.y - 1) / block.y, a.g.nz);
+        }
     }
     if (L == nullptr) return fail(LBM_E_UNSUPPORTED, "no kernel for this storage type / pattern");
     cudaError_t e = L(a, grid, block, stream);
