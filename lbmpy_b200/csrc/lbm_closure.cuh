@@ -163,129 +163,148 @@ LBM_HD R closure_nu_t(const R (&x)[MLP_IN], const WA& w) {
 
 #ifdef __CUDACC__
 // ------------------------------------------------------------------ tensor-core inference (FP32)
-// The network for the 32 cells of a warp at once: each layer is a 32 x K by K x 32 product done
-// as m16n8k8 TF32 tiles (mma.sync; rows are the warp's cells), the hidden activations pass
-// through a per-warp shared-memory tile of 32 rows.  TF32 operands (10-bit mantissa) give nu_t to
-// about 1e-3 relative; training and the FP64 sweep use the exact network.
+// The network for the 32 cells of a warp at once, as three chained m16n8k16 FP16 products with
+// FP32 accumulation (mma.sync; rows are the warp's cells, taken 16 at a time): [16 x 16]
+// features (zero-padded from 10) x [16 x 32], [16 x 32] x [32 x 32], [16 x 32] x [32 x 8] (the
+// output unit in column 0).  The accumulator fragment of one product has the layout of the A
+// fragment of the next (two adjacent 8-column tiles form one 16-wide k-step), so the hidden
+// activations never leave registers: bias, SiLU and the FP16 packing are applied in place.  Only
+// the features pass through shared memory once, to be transposed into A fragments.  FP16 operands
+// (11-bit significand, as TF32) give nu_t to about 1e-3 relative; training and the FP64 sweep use
+// the exact network.
 
-constexpr int MLP_TLD = 33;                       // row stride of the per-warp activation tile
+constexpr int MLP_FRAGS = 4 + 8 + 2;             // B fragments: layer 1 (4 n-tiles), 2 (2 k x 4 n), 3 (2 k)
+constexpr int MLP_XLD = 12;                      // row stride (32-bit words) of a warp's feature tile
 
-__device__ __forceinline__ uint32_t to_tf32(float v) {
+// Shared-memory image of the parameters: per B fragment and lane the two 32-bit registers of
+// mma.m16n8k16's B operand (f16 pairs along k), the halved biases of both hidden layers, b3 and
+// the output scale.
+struct MlpShared {
+    uint2 frag[MLP_FRAGS][32];
+    float hb1[MLP_H], hb2[MLP_H];
+    float b3, scale;
+};
+
+__device__ __forceinline__ uint32_t pack_half2(float lo, float hi) {
     uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
     return r;
 }
 
-__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                         uint32_t b0, uint32_t b1) {
-    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-                 "{%0,%1,%2,%3};"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+// SiLU of two pre-activations given as h = z / 2: h (1 + tanh h) in packed FP16, with the
+// hardware tanh (tanh.approx.f16x2).  The result is one A-fragment register of the next product.
+__device__ __forceinline__ uint32_t silu_half2(float h_lo, float h_hi) {
+    uint32_t r;
+    asm("{\n\t.reg .b32 h, t;\n\t"
+        "cvt.rn.f16x2.f32 h, %2, %1;\n\t"
+        "tanh.approx.f16x2 t, h;\n\t"
+        "fma.rn.f16x2 %0, h, t, h;\n\t}"
+        : "=r"(r) : "f"(h_lo), "f"(h_hi));
+    return r;
 }
 
-// Parameter block as the tensor-core network reads it from shared memory: the entries of W1 and
-// W2 as TF32 bit patterns, everything else as FP32 bit patterns.
+__device__ __forceinline__ void mma_f16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                        uint2 b) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b.x), "r"(b.y));
+}
+
+// Fills `s` from the FP32 parameter block; all threads of the block take part.  Fragment f, lane
+// (g = lane / 4, t = lane % 4) holds rows k0 = 16 ks + 2t, k0 + 1 (first register) and k0 + 8,
+// k0 + 9 (second) of column n = 8 nt + g of the layer's K x N weight matrix.
 template <class WA>
-__device__ __forceinline__ void stage_mlp_params(const WA& w, uint32_t* sw, int tid, int nthreads) {
-    for (int i = tid; i < MLP_PARAMS; i += nthreads) {
-        const float v = w[i];
-        const bool matrix = i < MLP_B1 || (i >= MLP_W2 && i < MLP_B2);
-        sw[i] = matrix ? to_tf32(v) : __float_as_uint(v);
+__device__ __forceinline__ void stage_mlp_params(const WA& w, MlpShared& s, int tid, int nthreads) {
+    for (int i = tid; i < MLP_FRAGS * 32; i += nthreads) {
+        const int f = i >> 5, lane = i & 31, g = lane >> 2, t = lane & 3;
+        float v[4];
+        if (f < 4) {                                   // layer 1: W1[k][n], k < MLP_IN
+            const int n = 8 * f + g;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int k = 2 * t + (j & 1) + 8 * (j >> 1);
+                v[j] = k < MLP_IN ? w[MLP_W1 + k * MLP_H + n] : 0.f;
+            }
+        } else if (f < 12) {                           // layer 2: W2[k][n]
+            const int ks = (f - 4) >> 2, n = 8 * ((f - 4) & 3) + g;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = w[MLP_W2 + (16 * ks + 2 * t + (j & 1) + 8 * (j >> 1)) * MLP_H + n];
+        } else {                                       // output unit in column 0
+            const int ks = f - 12;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = g == 0 ? w[MLP_W3 + 16 * ks + 2 * t + (j & 1) + 8 * (j >> 1)] : 0.f;
+        }
+        s.frag[f][lane] = make_uint2(pack_half2(v[0], v[1]), pack_half2(v[2], v[3]));
+    }
+    for (int i = tid; i < MLP_H; i += nthreads) {
+        s.hb1[i] = 0.5f * w[MLP_B1 + i];
+        s.hb2[i] = 0.5f * w[MLP_B2 + i];
+    }
+    if (tid == 0) {
+        s.b3 = w[MLP_B3];
+        s.scale = w[MLP_SCALE];
     }
 }
 
-// nu_t of this lane's cell; every lane of the warp must call it together.  T: this warp's
-// 32 x MLP_TLD float tile.
-__device__ __forceinline__ float warp_mlp_nu(const float (&x)[MLP_IN], const uint32_t* sw, float* T) {
+// Bias + SiLU of two adjacent 8-column accumulator tiles (columns 16 ks .. 16 ks + 15 of a hidden
+// layer) into the four A-fragment registers of the next product's k-step ks.
+__device__ __forceinline__ void hidden_to_a(const float (&lo)[4], const float (&hi)[4], const float* hb, int ks,
+                                            int t, uint32_t (&a)[4]) {
+    const float2 bl = *reinterpret_cast<const float2*>(hb + 16 * ks + 2 * t);
+    const float2 bh = *reinterpret_cast<const float2*>(hb + 16 * ks + 8 + 2 * t);
+    a[0] = silu_half2(fmaf(lo[0], 0.5f, bl.x), fmaf(lo[1], 0.5f, bl.y));
+    a[1] = silu_half2(fmaf(lo[2], 0.5f, bl.x), fmaf(lo[3], 0.5f, bl.y));
+    a[2] = silu_half2(fmaf(hi[0], 0.5f, bh.x), fmaf(hi[1], 0.5f, bh.y));
+    a[3] = silu_half2(fmaf(hi[2], 0.5f, bh.x), fmaf(hi[3], 0.5f, bh.y));
+}
+
+// nu_t of this lane's cell; every lane of the warp must call it together.  X: this warp's feature
+// tile, 32 rows of MLP_XLD words.
+__device__ __forceinline__ float warp_mlp_nu(const float (&x)[MLP_IN], const MlpShared& s, uint32_t* X) {
     const int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
-    const int gid = lane >> 2, t4 = lane & 3;
-    auto F = [&](int i) { return __uint_as_float(sw[i]); };
-#pragma unroll
-    for (int k = 0; k < 16; ++k) T[lane * MLP_TLD + k] = k < MLP_IN ? x[k] : 0.f;
+    const int g = lane >> 2, t = lane & 3;
+    {
+        uint4* row = reinterpret_cast<uint4*>(X + lane * MLP_XLD);
+        row[0] = make_uint4(pack_half2(x[0], x[1]), pack_half2(x[2], x[3]), pack_half2(x[4], x[5]),
+                            pack_half2(x[6], x[7]));
+        row[1] = make_uint4(pack_half2(x[8], x[9]), 0u, 0u, 0u);
+    }
     __syncwarp();
-    float acc[2][4][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[mt][nt][c] = 0.f;
-    // layer 1: [32 x 16] (features, zero-padded) x [16 x 32]
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int ks = 0; ks < 2; ++ks) {
-            const int r0 = (mt * 16 + gid) * MLP_TLD, r1 = r0 + 8 * MLP_TLD, c0 = ks * 8 + t4;
-            const uint32_t a0 = to_tf32(T[r0 + c0]), a1 = to_tf32(T[r1 + c0]);
-            const uint32_t a2 = to_tf32(T[r0 + c0 + 4]), a3 = to_tf32(T[r1 + c0 + 4]);
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                const int n = nt * 8 + gid;
-                const uint32_t b0 = c0 < MLP_IN ? sw[MLP_W1 + c0 * MLP_H + n] : 0u;
-                const uint32_t b1 = c0 + 4 < MLP_IN ? sw[MLP_W1 + (c0 + 4) * MLP_H + n] : 0u;
-                mma_tf32(acc[mt][nt], a0, a1, a2, a3, b0, b1);
-            }
-        }
-    __syncwarp();
-    // bias + SiLU, back into the tile as rows of 32 hidden units
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
+    float y = 0.f;
+#pragma unroll 1
+    for (int mt = 0; mt < 2; ++mt) {
+        const uint32_t* r0 = X + (16 * mt + g) * MLP_XLD + t;
+        const uint32_t* r1 = r0 + 8 * MLP_XLD;
+        const uint32_t a0 = r0[0], a1 = r1[0], a2 = r0[4], a3 = r1[4];
+        float h1[4][4];
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
-            const int col = nt * 8 + 2 * t4, r0 = (mt * 16 + gid) * MLP_TLD, r1 = r0 + 8 * MLP_TLD;
-            const float blo = F(MLP_B1 + col), bhi = F(MLP_B1 + col + 1);
-            T[r0 + col] = mlp_silu_sweep<float>(acc[mt][nt][0] + blo);
-            T[r0 + col + 1] = mlp_silu_sweep<float>(acc[mt][nt][1] + bhi);
-            T[r1 + col] = mlp_silu_sweep<float>(acc[mt][nt][2] + blo);
-            T[r1 + col + 1] = mlp_silu_sweep<float>(acc[mt][nt][3] + bhi);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[mt][nt][c] = 0.f;
+            h1[nt][0] = h1[nt][1] = h1[nt][2] = h1[nt][3] = 0.f;
+            mma_f16(h1[nt], a0, a1, a2, a3, s.frag[nt][lane]);
         }
-    __syncwarp();
-    // layer 2: [32 x 32] x [32 x 32]
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-            const int r0 = (mt * 16 + gid) * MLP_TLD, r1 = r0 + 8 * MLP_TLD, c0 = ks * 8 + t4;
-            const uint32_t a0 = to_tf32(T[r0 + c0]), a1 = to_tf32(T[r1 + c0]);
-            const uint32_t a2 = to_tf32(T[r0 + c0 + 4]), a3 = to_tf32(T[r1 + c0 + 4]);
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                const int n = nt * 8 + gid;
-                mma_tf32(acc[mt][nt], a0, a1, a2, a3, sw[MLP_W2 + c0 * MLP_H + n], sw[MLP_W2 + (c0 + 4) * MLP_H + n]);
-            }
-        }
-    // output unit: per-lane partial sums over its columns, then over the 4 lanes of a row group
-    float y[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
+        uint32_t a[2][4];
+        hidden_to_a(h1[0], h1[1], s.hb1, 0, t, a[0]);
+        hidden_to_a(h1[2], h1[3], s.hb1, 1, t, a[1]);
+        float h2[4][4];
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
-            const int col = nt * 8 + 2 * t4;
-            const float blo = F(MLP_B2 + col), bhi = F(MLP_B2 + col + 1);
-            const float wlo = F(MLP_W3 + col), whi = F(MLP_W3 + col + 1);
-            y[mt][0] += mlp_silu_sweep<float>(acc[mt][nt][0] + blo) * wlo +
-                        mlp_silu_sweep<float>(acc[mt][nt][1] + bhi) * whi;
-            y[mt][1] += mlp_silu_sweep<float>(acc[mt][nt][2] + blo) * wlo +
-                        mlp_silu_sweep<float>(acc[mt][nt][3] + bhi) * whi;
-        }
+            h2[nt][0] = h2[nt][1] = h2[nt][2] = h2[nt][3] = 0.f;
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            y[mt][h] += __shfl_xor_sync(0xffffffffu, y[mt][h], 1);
-            y[mt][h] += __shfl_xor_sync(0xffffffffu, y[mt][h], 2);
+            for (int ks = 0; ks < 2; ++ks) mma_f16(h2[nt], a[ks][0], a[ks][1], a[ks][2], a[ks][3], s.frag[4 + 4 * ks + nt][lane]);
         }
-    // row `lane` sits in tile lane >> 4, half (lane >> 3) & 1, row group lane & 7
-    const int src = 4 * (lane & 7);
-    const float v00 = __shfl_sync(0xffffffffu, y[0][0], src), v01 = __shfl_sync(0xffffffffu, y[0][1], src);
-    const float v10 = __shfl_sync(0xffffffffu, y[1][0], src), v11 = __shfl_sync(0xffffffffu, y[1][1], src);
-    const int mt = lane >> 4, half = (lane >> 3) & 1;
-    const float yv = (mt ? (half ? v11 : v10) : (half ? v01 : v00)) + F(MLP_B3);
+        hidden_to_a(h2[0], h2[1], s.hb2, 0, t, a[0]);
+        hidden_to_a(h2[2], h2[3], s.hb2, 1, t, a[1]);
+        float o[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) mma_f16(o, a[ks][0], a[ks][1], a[ks][2], a[ks][3], s.frag[12 + ks][lane]);
+        // column 0: lane 4r holds the outputs of rows r (o[0]) and r + 8 (o[2]) of this tile
+        const int src = 4 * (lane & 7);
+        const float lo = __shfl_sync(0xffffffffu, o[0], src), hi = __shfl_sync(0xffffffffu, o[2], src);
+        if ((lane >> 4) == mt) y = (lane & 8) ? hi : lo;
+    }
     __syncwarp();
-    return F(MLP_SCALE) * mlp_softplus<float>(yv);
+    return s.scale * mlp_softplus<float>(y + s.b3);
 }
 #endif
 

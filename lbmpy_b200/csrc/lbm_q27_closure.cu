@@ -25,13 +25,13 @@ template <class R> struct ClosureNu {
 
 // FP32: the network of the warp's 32 cells on the tensor cores (warp_mlp_nu).
 struct WarpClosureNu {
-    const uint32_t* sw;
-    float* T;
+    const MlpShared* s;
+    uint32_t* X;
     __device__ __forceinline__ float operator()(float pxx, float pyy, float pzz, float pxy, float pxz, float pyz,
                                                 float rho, float ux, float uy, float uz) const {
         float x[MLP_IN];
         closure_features<float>(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz, x);
-        return warp_mlp_nu(x, sw, T);
+        return warp_mlp_nu(x, *s, X);
     }
 };
 
@@ -40,14 +40,14 @@ struct WarpClosureNu {
 // values; only fluid cells inside the domain store.  Each thread sweeps a.zc consecutive planes
 // (amortising the parameter staging) and prefetches the next plane to L2.  Otherwise as k_sweep.
 template <int PAT>
-__global__ void __launch_bounds__(256) k_sweep_closure_tc(const SweepArgs a) {
+__global__ void __launch_bounds__(256, 3) k_sweep_closure_tc(const SweepArgs a) {
     using A = Access<PAT>;
-    __shared__ uint32_t sw[MLP_PARAMS];
-    __shared__ float tiles[8][32 * MLP_TLD];
+    __shared__ MlpShared sp;
+    __shared__ __align__(16) uint32_t tiles[8][32 * MLP_XLD];
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-    stage_mlp_params(ConstClosureWeights{}, sw, tid, blockDim.x * blockDim.y);
+    stage_mlp_params(ConstClosureWeights{}, sp, tid, blockDim.x * blockDim.y);
     __syncthreads();
-    const WarpClosureNu nu{sw, tiles[tid >> 5]};
+    const WarpClosureNu nu{&sp, tiles[tid >> 5]};
     const Grid& g = a.g;
     const int xr = blockIdx.x * blockDim.x + threadIdx.x;
     const int yr = blockIdx.y * blockDim.y + threadIdx.y;
