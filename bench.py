@@ -210,16 +210,19 @@ class SparsePorousMedium:
 WORKLOADS["sparse-porous-192-d3q19-trt-float32"] = (lambda dev: SparsePorousMedium(dev), None, 19, 4)
 
 
-def make_closure_box(device, shape=(256, 128, 128)):
+def make_closure_box(device, shape=(256, 128, 128), closure=True):
     """D3Q27 cumulant (omega 1.99) with the learned closure, FP32, AA, periodic box; the network
-    is a seeded untrained one (its cost does not depend on the parameter values)."""
+    is a seeded untrained one (its cost does not depend on the parameter values).  closure=False:
+    the same box with the plain method, the closure's cost reference."""
     import lbmpy_b200 as L
     from lbmpy_b200.closure import MLPClosure
-    clo = MLPClosure(seed=0, nu_scale=3e-4, device=device)
+    kw = {}
+    if closure:
+        kw["subgrid_scale_model"] = (L.SubgridScaleModel.LEARNED, MLPClosure(seed=0, nu_scale=3e-4, device=device))
     step = L.LatticeBoltzmannStep(domain_size=shape, periodicity=True, stencil=L.Stencil.D3Q27,
                                   method=L.Method.CUMULANT, relaxation_rate=1.99, compressible=True,
                                   streaming_pattern="aa", config=L.CreateKernelConfig(data_type="float32"),
-                                  subgrid_scale_model=(L.SubgridScaleModel.LEARNED, clo), device=device)
+                                  device=device, **kw)
     rng = np.random.default_rng(0)
     step.velocity_array[...] = rng.uniform(-0.02, 0.02, shape + (3,)).astype(np.float32)
     step.set_pdf_fields_from_macroscopic_values()
@@ -227,6 +230,7 @@ def make_closure_box(device, shape=(256, 128, 128)):
 
 
 WORKLOADS["d3q27-cumulant-closure-aa-periodic-256x128x128"] = (lambda dev: make_closure_box(dev), None, 27, 4)
+WORKLOADS["d3q27-cumulant-aa-periodic-256x128x128"] = (lambda dev: make_closure_box(dev, closure=False), None, 27, 4)
 
 
 def make_channel(device, shape=SHAPE, seed=0):

@@ -90,17 +90,42 @@ template <class R> LBM_HD R mlp_silu_sweep(R z) {
 //  7 (Pi_xy^2 + Pi_xz^2 + Pi_yz^2) / |Pi|^2 (off-diagonal fraction, lattice-frame)
 //  8 max_i |dev(Pi)_ii| / |dev(Pi)|
 //  9 1000 |u|^2
-template <class R>
+//
+// FAST (the FP32 sweep, whose network rounds the features to FP16 anyway): square roots, quotients
+// and the logarithm with the hardware approximations (relative error about 2^-21).
+template <class R, bool FAST = false>
 LBM_HD void closure_features(R pxx, R pyy, R pzz, R pxy, R pxz, R pyz, R rho, R ux, R uy, R uz,
                              R (&x)[MLP_IN]) {
+    auto sq = [](R v) -> R {
+#ifdef __CUDA_ARCH__
+        if constexpr (FAST && std::is_same<R, float>::value) {
+            float r;
+            asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(v));
+            return r;
+        }
+#endif
+        return mlp_sqrt<R>(v);
+    };
+    auto dv = [](R a, R b) -> R {
+#ifdef __CUDA_ARCH__
+        if constexpr (FAST && std::is_same<R, float>::value) return __fdividef(a, b);
+#endif
+        return a / b;
+    };
+    auto lg = [](R v) -> R {
+#ifdef __CUDA_ARCH__
+        if constexpr (FAST && std::is_same<R, float>::value) return __logf(v);
+#endif
+        return mlp_log<R>(v);
+    };
     const R off2 = pxy * pxy + pxz * pxz + pyz * pyz;
     const R s2 = pxx * pxx + pyy * pyy + pzz * pzz + R(2) * off2;
-    const R pim = mlp_sqrt<R>(R(2) * s2) / rho;
+    const R pim = dv(sq(R(2) * s2), rho);
     const R tr = pxx + pyy + pzz;
     const R t3 = tr * R(1.0 / 3.0);
     const R dxx = pxx - t3, dyy = pyy - t3, dzz = pzz - t3;
     const R d2 = dxx * dxx + dyy * dyy + dzz * dzz + R(2) * off2;
-    const R dn = mlp_sqrt<R>(d2);
+    const R dn = sq(d2);
     const R tr3 = dxx * dxx * dxx + dyy * dyy * dyy + dzz * dzz * dzz +
                   R(3) * (dxx * (pxy * pxy + pxz * pxz) + dyy * (pxy * pxy + pyz * pyz) +
                           dzz * (pxz * pxz + pyz * pyz)) +
@@ -111,15 +136,15 @@ LBM_HD void closure_features(R pxx, R pyy, R pzz, R pxy, R pxz, R pyz, R rho, R 
     R mx = mlp_abs<R>(dxx);
     if (mlp_abs<R>(dyy) > mx) mx = mlp_abs<R>(dyy);
     if (mlp_abs<R>(dzz) > mx) mx = mlp_abs<R>(dzz);
-    x[0] = mlp_log<R>(pim + R(1e-9));
+    x[0] = lg(pim + R(1e-9));
     x[1] = R(100) * pim;
-    x[2] = tr / (mlp_sqrt<R>(s2) + R(1e-12));
-    x[3] = R(2.449489742783178) * tr3 / (d2 * dn + R(1e-30));
-    x[4] = R(30) * mlp_sqrt<R>(u2);
+    x[2] = dv(tr, sq(s2) + R(1e-12));
+    x[3] = dv(R(2.449489742783178) * tr3, d2 * dn + R(1e-30));
+    x[4] = R(30) * sq(u2);
     x[5] = R(1000) * (rho - R(1));
-    x[6] = uau / ((u2 + R(1e-12)) * dn + R(1e-30));
-    x[7] = off2 / (s2 + R(1e-30));
-    x[8] = mx / (dn + R(1e-30));
+    x[6] = dv(uau, (u2 + R(1e-12)) * dn + R(1e-30));
+    x[7] = dv(off2, s2 + R(1e-30));
+    x[8] = dv(mx, dn + R(1e-30));
     x[9] = R(1000) * u2;
 }
 
@@ -163,27 +188,34 @@ LBM_HD R closure_nu_t(const R (&x)[MLP_IN], const WA& w) {
 
 #ifdef __CUDACC__
 // ------------------------------------------------------------------ tensor-core inference (FP32)
-// The network for the 32 cells of a warp at once, as three chained m16n8k16 FP16 products with
-// FP32 accumulation (mma.sync; rows are the warp's cells, taken 16 at a time): [16 x 16]
-// features (zero-padded from 10) x [16 x 32], [16 x 32] x [32 x 32], [16 x 32] x [32 x 8] (the
-// output unit in column 0).  The accumulator fragment of one product has the layout of the A
-// fragment of the next (two adjacent 8-column tiles form one 16-wide k-step), so the hidden
-// activations never leave registers: bias, SiLU and the FP16 packing are applied in place.  Only
-// the features pass through shared memory once, to be transposed into A fragments.  FP16 operands
-// (11-bit significand, as TF32) give nu_t to about 1e-3 relative; training and the FP64 sweep use
-// the exact network.
+// The network for the 32 cells of a warp at once, as three chained m16n8k16 FP16 products
+// (mma.sync; rows are the warp's cells, taken 16 at a time): [16 x 16] features (zero-padded
+// from 10) x [16 x 32], [16 x 32] x [32 x 32], [16 x 32] x [32 x 8] (the output unit in column
+// 0), accumulating in FP32 from the biases.  The accumulator fragment of a hidden layer has the
+// layout of the A fragment of the next product (two adjacent 8-column tiles form one 16-wide
+// k-step), so the hidden activations never leave registers: the SiLU and the FP16 packing are
+// applied to them in place.  Only the features pass through shared memory once, to be
+// transposed into A fragments.  FP16 operands (11-bit significand, as TF32) give nu_t to about
+// 1e-3 relative; training and the FP64 sweep use the exact network.
 
 constexpr int MLP_FRAGS = 4 + 8 + 2;             // B fragments: layer 1 (4 n-tiles), 2 (2 k x 4 n), 3 (2 k)
 constexpr int MLP_XLD = 12;                      // row stride (32-bit words) of a warp's feature tile
 
 // Shared-memory image of the parameters: per B fragment and lane the two 32-bit registers of
-// mma.m16n8k16's B operand (f16 pairs along k), the halved biases of both hidden layers, b3 and
-// the output scale.
-struct MlpShared {
+// mma.m16n8k16's B operand (f16 pairs along k), the halved biases of both hidden layers as
+// accumulator start values, b3 and the output scale.  Copied in 16-byte pieces.
+struct __align__(16) MlpShared {
     uint2 frag[MLP_FRAGS][32];
-    float hb1[MLP_H], hb2[MLP_H];
+    float4 hb1[4][4], hb2[4][4];   // [n-tile][t]: halved biases of columns 8 nt + 2t, + 1, twice
     float b3, scale;
+    float pad_[2];
 };
+
+// Softplus for the in-sweep FP32 inference, with the fast exponential and logarithm (absolute
+// error of log(1 + e^y) about 1e-7).
+__device__ __forceinline__ float mlp_softplus_sweep(float y) {
+    return y > 20.f ? y : __logf(1.f + __expf(y));
+}
 
 __device__ __forceinline__ uint32_t pack_half2(float lo, float hi) {
     uint32_t r;
@@ -213,7 +245,9 @@ __device__ __forceinline__ void mma_f16(float (&d)[4], uint32_t a0, uint32_t a1,
 
 // Fills `s` from the FP32 parameter block; all threads of the block take part.  Fragment f, lane
 // (g = lane / 4, t = lane % 4) holds rows k0 = 16 ks + 2t, k0 + 1 (first register) and k0 + 8,
-// k0 + 9 (second) of column n = 8 nt + g of the layer's K x N weight matrix.
+// k0 + 9 (second) of column n = 8 nt + g of the layer's K x N weight matrix.  The hidden layers'
+// weights and biases are stored halved (exact in FP16), so that their products give h = z / 2,
+// the argument of the SiLU's tanh, directly.
 template <class WA>
 __device__ __forceinline__ void stage_mlp_params(const WA& w, MlpShared& s, int tid, int nthreads) {
     for (int i = tid; i < MLP_FRAGS * 32; i += nthreads) {
@@ -224,12 +258,12 @@ __device__ __forceinline__ void stage_mlp_params(const WA& w, MlpShared& s, int 
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int k = 2 * t + (j & 1) + 8 * (j >> 1);
-                v[j] = k < MLP_IN ? w[MLP_W1 + k * MLP_H + n] : 0.f;
+                v[j] = k < MLP_IN ? 0.5f * w[MLP_W1 + k * MLP_H + n] : 0.f;
             }
         } else if (f < 12) {                           // layer 2: W2[k][n]
             const int ks = (f - 4) >> 2, n = 8 * ((f - 4) & 3) + g;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) v[j] = w[MLP_W2 + (16 * ks + 2 * t + (j & 1) + 8 * (j >> 1)) * MLP_H + n];
+            for (int j = 0; j < 4; ++j) v[j] = 0.5f * w[MLP_W2 + (16 * ks + 2 * t + (j & 1) + 8 * (j >> 1)) * MLP_H + n];
         } else {                                       // output unit in column 0
             const int ks = f - 12;
 #pragma unroll
@@ -237,9 +271,12 @@ __device__ __forceinline__ void stage_mlp_params(const WA& w, MlpShared& s, int 
         }
         s.frag[f][lane] = make_uint2(pack_half2(v[0], v[1]), pack_half2(v[2], v[3]));
     }
-    for (int i = tid; i < MLP_H; i += nthreads) {
-        s.hb1[i] = 0.5f * w[MLP_B1 + i];
-        s.hb2[i] = 0.5f * w[MLP_B2 + i];
+    for (int i = tid; i < 16; i += nthreads) {
+        const int col = 8 * (i >> 2) + 2 * (i & 3);
+        const float a0 = 0.5f * w[MLP_B1 + col], a1 = 0.5f * w[MLP_B1 + col + 1];
+        const float c0 = 0.5f * w[MLP_B2 + col], c1 = 0.5f * w[MLP_B2 + col + 1];
+        s.hb1[i >> 2][i & 3] = make_float4(a0, a1, a0, a1);
+        s.hb2[i >> 2][i & 3] = make_float4(c0, c1, c0, c1);
     }
     if (tid == 0) {
         s.b3 = w[MLP_B3];
@@ -247,16 +284,13 @@ __device__ __forceinline__ void stage_mlp_params(const WA& w, MlpShared& s, int 
     }
 }
 
-// Bias + SiLU of two adjacent 8-column accumulator tiles (columns 16 ks .. 16 ks + 15 of a hidden
-// layer) into the four A-fragment registers of the next product's k-step ks.
-__device__ __forceinline__ void hidden_to_a(const float (&lo)[4], const float (&hi)[4], const float* hb, int ks,
-                                            int t, uint32_t (&a)[4]) {
-    const float2 bl = *reinterpret_cast<const float2*>(hb + 16 * ks + 2 * t);
-    const float2 bh = *reinterpret_cast<const float2*>(hb + 16 * ks + 8 + 2 * t);
-    a[0] = silu_half2(fmaf(lo[0], 0.5f, bl.x), fmaf(lo[1], 0.5f, bl.y));
-    a[1] = silu_half2(fmaf(lo[2], 0.5f, bl.x), fmaf(lo[3], 0.5f, bl.y));
-    a[2] = silu_half2(fmaf(hi[0], 0.5f, bh.x), fmaf(hi[1], 0.5f, bh.y));
-    a[3] = silu_half2(fmaf(hi[2], 0.5f, bh.x), fmaf(hi[3], 0.5f, bh.y));
+// SiLU of two adjacent 8-column accumulator tiles (h = z / 2 of columns 16 ks .. 16 ks + 15 of a
+// hidden layer) into the four A-fragment registers of the next product's k-step ks.
+__device__ __forceinline__ void hidden_to_a(const float (&lo)[4], const float (&hi)[4], uint32_t (&a)[4]) {
+    a[0] = silu_half2(lo[0], lo[1]);
+    a[1] = silu_half2(lo[2], lo[3]);
+    a[2] = silu_half2(hi[0], hi[1]);
+    a[3] = silu_half2(hi[2], hi[3]);
 }
 
 // nu_t of this lane's cell; every lane of the warp must call it together.  X: this warp's feature
@@ -277,25 +311,28 @@ __device__ __forceinline__ float warp_mlp_nu(const float (&x)[MLP_IN], const Mlp
         const uint32_t* r0 = X + (16 * mt + g) * MLP_XLD + t;
         const uint32_t* r1 = r0 + 8 * MLP_XLD;
         const uint32_t a0 = r0[0], a1 = r1[0], a2 = r0[4], a3 = r1[4];
+        // accumulators start at the halved biases (one 16-byte shared load per tile)
         float h1[4][4];
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
-            h1[nt][0] = h1[nt][1] = h1[nt][2] = h1[nt][3] = 0.f;
+            const float4 b = s.hb1[nt][t];
+            h1[nt][0] = b.x; h1[nt][1] = b.y; h1[nt][2] = b.z; h1[nt][3] = b.w;
             mma_f16(h1[nt], a0, a1, a2, a3, s.frag[nt][lane]);
         }
         uint32_t a[2][4];
-        hidden_to_a(h1[0], h1[1], s.hb1, 0, t, a[0]);
-        hidden_to_a(h1[2], h1[3], s.hb1, 1, t, a[1]);
+        hidden_to_a(h1[0], h1[1], a[0]);
+        hidden_to_a(h1[2], h1[3], a[1]);
         float h2[4][4];
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
-            h2[nt][0] = h2[nt][1] = h2[nt][2] = h2[nt][3] = 0.f;
+            const float4 b = s.hb2[nt][t];
+            h2[nt][0] = b.x; h2[nt][1] = b.y; h2[nt][2] = b.z; h2[nt][3] = b.w;
 #pragma unroll
             for (int ks = 0; ks < 2; ++ks) mma_f16(h2[nt], a[ks][0], a[ks][1], a[ks][2], a[ks][3], s.frag[4 + 4 * ks + nt][lane]);
         }
-        hidden_to_a(h2[0], h2[1], s.hb2, 0, t, a[0]);
-        hidden_to_a(h2[2], h2[3], s.hb2, 1, t, a[1]);
-        float o[4] = {0.f, 0.f, 0.f, 0.f};
+        hidden_to_a(h2[0], h2[1], a[0]);
+        hidden_to_a(h2[2], h2[3], a[1]);
+        float o[4] = {s.b3, 0.f, s.b3, 0.f};
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) mma_f16(o, a[ks][0], a[ks][1], a[ks][2], a[ks][3], s.frag[12 + ks][lane]);
         // column 0: lane 4r holds the outputs of rows r (o[0]) and r + 8 (o[2]) of this tile
@@ -304,7 +341,7 @@ __device__ __forceinline__ float warp_mlp_nu(const float (&x)[MLP_IN], const Mlp
         if ((lane >> 4) == mt) y = (lane & 8) ? hi : lo;
     }
     __syncwarp();
-    return s.scale * mlp_softplus<float>(y + s.b3);
+    return s.scale * mlp_softplus_sweep(y);
 }
 #endif
 

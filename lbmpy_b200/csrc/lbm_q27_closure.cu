@@ -7,6 +7,9 @@
 namespace lbm {
 
 static __constant__ float c_closure[MLP_PARAMS];
+// The parameters as the FP32 sweep's tensor-core network reads them (stage_mlp_params), built
+// once per upload; each sweep block copies it into shared memory with 16-byte loads.
+static __device__ MlpShared g_closure_image;
 
 // Reads the parameters by name, so that the unrolled network addresses constant memory directly.
 struct ConstClosureWeights {
@@ -30,7 +33,7 @@ struct WarpClosureNu {
     __device__ __forceinline__ float operator()(float pxx, float pyy, float pzz, float pxy, float pxz, float pyz,
                                                 float rho, float ux, float uy, float uz) const {
         float x[MLP_IN];
-        closure_features<float>(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz, x);
+        closure_features<float, true>(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz, x);
         return warp_mlp_nu(x, *s, X);
     }
 };
@@ -45,7 +48,9 @@ __global__ void __launch_bounds__(256, 3) k_sweep_closure_tc(const SweepArgs a) 
     __shared__ MlpShared sp;
     __shared__ __align__(16) uint32_t tiles[8][32 * MLP_XLD];
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-    stage_mlp_params(ConstClosureWeights{}, sp, tid, blockDim.x * blockDim.y);
+    static_assert(sizeof(MlpShared) % 16 == 0, "the image is copied in 16-byte pieces");
+    for (int i = tid; i < int(sizeof(MlpShared) / 16); i += blockDim.x * blockDim.y)
+        reinterpret_cast<uint4*>(&sp)[i] = reinterpret_cast<const uint4*>(&g_closure_image)[i];
     __syncthreads();
     const WarpClosureNu nu{&sp, tiles[tid >> 5]};
     const Grid& g = a.g;
@@ -110,9 +115,16 @@ SweepLauncher sweep_q27_closure(int store, int pat) {
     return nullptr;
 }
 
+__global__ void __launch_bounds__(256) k_closure_image() {
+    stage_mlp_params(ConstClosureWeights{}, g_closure_image, threadIdx.x, blockDim.x);
+}
+
 cudaError_t closure_upload(const float* host_params, cudaStream_t stream) {
-    return cudaMemcpyToSymbolAsync(c_closure, host_params, sizeof(float) * MLP_PARAMS, 0, cudaMemcpyHostToDevice,
-                                   stream);
+    cudaError_t e = cudaMemcpyToSymbolAsync(c_closure, host_params, sizeof(float) * MLP_PARAMS, 0,
+                                            cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+    k_closure_image<<<1, 256, 0, stream>>>();
+    return cudaGetLastError();
 }
 
 }  // namespace lbm

@@ -400,8 +400,8 @@ class SparseSetter:
         dens = self.density if density is None else density
         vel = self.velocity if velocity is None else velocity
         dev = pdfs.device
-        rho = torch.as_tensor(np.broadcast_to(np.asarray(1.0 if dens is True else dens, dtype=np.float64), (n,)),
-                              device=dev).contiguous()
+        rho = torch.as_tensor(np.array(np.broadcast_to(np.asarray(1.0 if dens is True else dens, dtype=np.float64),
+                                                       (n,))), device=dev)
         v = np.asarray((0.0, 0.0, 0.0) if vel is True else vel, dtype=np.float64)
         u = torch.as_tensor(np.ascontiguousarray(np.broadcast_to(v, (n, 3)).T), device=dev)
         plan = self._plans.plan(_store_name(pdfs.dtype), {})
