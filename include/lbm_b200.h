@@ -219,7 +219,8 @@ int lbm_flags_finalize(const LbmPlan* plan, uint8_t* flags, void* stream);
  * values, W1[10][32] b1[32] W2[32][32] b2[32] W3[32] b3 scale (nu_t = scale * softplus(y)). */
 
 /* Uploads the parameters (host memory) that every closure sweep on the current device reads;
- * one set per device and process, ordered on `stream` before later launches. */
+ * one set per device and process, ordered on `stream` before later launches.  A one-block kernel
+ * on the same stream then packs them into the FP16 fragment layout the FP32 sweep reads. */
 int lbm_closure_set_weights(const float* params, int n, void* stream);
 /* Features of n cells from their state, SoA [10][n] device arrays: Pi_xx Pi_yy Pi_zz Pi_xy
  * Pi_xz Pi_yz (pre-collision non-equilibrium stress), rho, ux, uy, uz -> feats [10][n]. */
