@@ -215,12 +215,17 @@ __device__ __forceinline__ void sweep_cell(const SweepArgs& a, int x, int y, int
 // Resident 256-thread blocks per SM that the one-cell sweep is compiled for.  The register
 // allocator otherwise trades occupancy for registers in ways that move with unrelated code (the
 // near-wall path): the D3Q27 cumulant AA odd sweep went from 80 to 92 registers (3 to 2 blocks)
-// when the per-link boundary data arrived.  These hot variants are held to the register counts
-// at which they ran at HBM speed (-Xptxas -v): 80 (3 blocks), 64 (4) and 48 (5).
+// when the per-link boundary data arrived, and the D3Q19 TRT AA odd sweep took 88 (2 blocks, 0.72
+// of the copy bandwidth; 0.92 at 64).  These hot variants are held to register counts checked
+// for spills with -Xptxas -v: 80 (3 blocks), 64 (4) and 48 (5).
 template <class S, int Q, int MK, int PAT> struct SweepMinBlocks { static constexpr int value = 1; };
 template <> struct SweepMinBlocks<float, 27, MK_CUM1, PAT_AA_ODD> { static constexpr int value = 3; };
 template <> struct SweepMinBlocks<float, 27, MK_CUM1, PAT_AA_EVEN> { static constexpr int value = 4; };
 template <> struct SweepMinBlocks<float, 19, MK_POP, PAT_PULL> { static constexpr int value = 5; };
+template <> struct SweepMinBlocks<float, 19, MK_POP, PAT_AA_ODD> { static constexpr int value = 4; };
+template <> struct SweepMinBlocks<float, 19, MK_POP, PAT_AA_EVEN> { static constexpr int value = 4; };
+template <> struct SweepMinBlocks<float, 27, MK_POP, PAT_AA_ODD> { static constexpr int value = 3; };
+template <> struct SweepMinBlocks<float, 27, MK_POP, PAT_AA_EVEN> { static constexpr int value = 4; };
 template <> struct SweepMinBlocks<float, 19, MK_MRT, PAT_PULL> { static constexpr int value = 4; };
 template <> struct SweepMinBlocks<float, 27, MK_MRT, PAT_PULL> { static constexpr int value = 3; };
 
