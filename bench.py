@@ -231,15 +231,19 @@ def make_closure_box(device, shape=(256, 128, 128), closure=True):
 
 WORKLOADS["d3q27-cumulant-closure-aa-periodic-256x128x128"] = (lambda dev: make_closure_box(dev), None, 27, 4)
 WORKLOADS["d3q27-cumulant-aa-periodic-256x128x128"] = (lambda dev: make_closure_box(dev, closure=False), None, 27, 4)
+WORKLOADS["d3q27-trt-aa-channel-256x128x128"] = (lambda dev: make_channel(dev, method="trt"), SHAPE[0] * SHAPE[1] * SHAPE[2],
+                                                 27, 4)
 
 
-def make_channel(device, shape=SHAPE, seed=0):
-    """The channel through the lbmpy-compatible API (create_channel-style set-up, AA in place)."""
+def make_channel(device, shape=SHAPE, seed=0, method="cumulant"):
+    """The channel through the lbmpy-compatible API (create_channel-style set-up, AA in place).
+    method "trt": the same channel with the D3Q27 TRT method instead of the cumulant one."""
     import lbmpy_b200 as L
+    kw = dict(galilean_correction=True) if method == "cumulant" else {}
     step = L.LatticeBoltzmannStep(domain_size=shape, periodicity=(True, False, False), stencil=L.Stencil.D3Q27,
-                                  method=L.Method.CUMULANT, relaxation_rate=OMEGA, compressible=True,
-                                  galilean_correction=True, force=(FORCE, 0, 0), streaming_pattern="aa",
-                                  config=L.CreateKernelConfig(data_type="float32"), device=device)
+                                  method=getattr(L.Method, method.upper()), relaxation_rate=OMEGA, compressible=True,
+                                  force=(FORCE, 0, 0), streaming_pattern="aa",
+                                  config=L.CreateKernelConfig(data_type="float32"), device=device, **kw)
     for d in ("N", "S", "T", "B"):
         step.boundary_handling.set_boundary(L.NoSlip(), L.slice_from_direction(d, 3))
     rng = np.random.default_rng(seed)
